@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark of the set-intersection hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sisi_large|sisi_plain|sisi_skewed] [--technique ip]
+
+One "step" is one pass of the single-pair (SISI) hot path over one pair of
+sets: the workload by default is |A| = |B| = 2^28 sorted unique uint32 drawn
+from [0, 2^31), intersect-path technique, count + materialised elements.
+Metric: Gelem/s = (|A| + |B|) / step time.
+
+  value   device-timed (CUDA events on the launching stream), inputs resident
+          in HBM; 2 GiB of input per step > 126 MB L2, so no L2 flush.
+  e2e     the same metric through the public host API (api.intersect_host):
+          pinned host sets -> H2D -> kernels -> count + elements D2H, per step.
+  roofline  live per-launch time of the dominant kernel (ip_tile) from the
+          library's phase timer over the timed region, against measured HBM.
+  cpu_baseline  the reference's own CPU executable (oracle/_ref/stdintersection,
+          built from the reference sources) on a bounded sample of the same
+          workload, timed by the reference's HostTimer.
+
+Multi-GPU: the single-pair path is replicas only -- each rank runs its own
+independent pair (no data-path collective); value is the whole-job aggregate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+CACHE_DIR = os.environ.get("SI_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "si_bench_cache"))
+
+WORKLOADS = {
+    "sisi_large": dict(desc="SISI |A|=|B|=2^28 uint32 uniform w/o replacement from [0,2^31), seeds 3,4",
+                       n=1 << 28, universe=1 << 31, seeds=(3, 4)),
+    "sisi_plain": dict(desc="SISI |A|=|B|=2^20 uint32 uniform w/o replacement from [0,2^24), seeds 1,2",
+                       n=1 << 20, universe=1 << 24, seeds=(1, 2)),
+    "sisi_skewed": dict(desc="SISI |A|=2^16, |B|=2^26 from [0,2^30), 20% of A planted into B, seed 5",
+                        n=None, universe=1 << 30, seeds=(5,)),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------- inputs --
+def make_pair(name: str):
+    from set_intersection_b200 import generate
+    os.makedirs(CACHE_DIR, exist_ok=True)
+    path = os.path.join(CACHE_DIR, f"{name}.npz")
+    if os.path.exists(path):
+        try:
+            z = np.load(path)
+            return z["a"], z["b"]
+        except Exception:
+            pass
+    w = WORKLOADS[name]
+    if name == "sisi_skewed":
+        a, b = generate.sisi_skewed(seed=w["seeds"][0])
+    else:
+        a = generate.uniform(w["seeds"][0], w["n"], w["universe"])
+        b = generate.uniform(w["seeds"][1], w["n"], w["universe"])
+    tmp = path + f".{os.getpid()}.tmp.npz"
+    np.savez(tmp, a=a, b=b)
+    os.replace(tmp, path)
+    return a, b
+
+
+def sample_pair(name: str, budget_elems: int):
+    """A bounded sample with the workload's density: |A'| = |B'| = n' drawn
+    from a universe scaled by n'/n (same per-element merge behaviour)."""
+    from set_intersection_b200 import generate
+    w = WORKLOADS[name]
+    if name == "sisi_skewed":
+        return make_pair(name), "full workload"
+    n = w["n"]
+    ns = int(min(n, max(1 << 16, budget_elems)))
+    ns = 1 << (ns.bit_length() - 1)
+    uni = int(w["universe"] * ns // n)
+    a = generate.uniform(w["seeds"][0] + 100, ns, uni)
+    b = generate.uniform(w["seeds"][1] + 100, ns, uni)
+    return (a, b), f"|A|=|B|=2^{ns.bit_length() - 1} from [0,2^{uni.bit_length() - 1}) (same density as the workload)"
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """Samples SM clock and clock-event reasons through NVML while running."""
+
+    REASONS = {
+        0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+        0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown", 0x2: "applications_clocks_setting",
+    }
+
+    def __init__(self, torch_dev: int = 0, period_s: float = 0.005):
+        self.period = period_s
+        self.samples, self.reasons = [], set()
+        self.ok = False
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            uuid = str(torch.cuda.get_device_properties(torch_dev).uuid)
+            try:
+                self.h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+            except Exception:
+                vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+                idx = int(vis.split(",")[torch_dev]) if vis and vis.split(",")[0].isdigit() else torch_dev
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception as e:  # pragma: no cover - depends on the box
+            log(f"clock sampling unavailable: {e}")
+            self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        nv = self.nvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self._t:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# -------------------------------------------------------------- reference --
+def reference_step_ms(a, b, tmpdir: str) -> float:
+    """One run of the reference's stdintersection on a 2-set dataset file; the
+    reference's own HostTimer figure for the intersection phase."""
+    import oracle
+    from set_intersection_b200 import dataset as fmt
+    path = os.path.join(tmpdir, "pair.bin")
+    if not os.path.exists(path):
+        fmt.write_dataset(path, fmt.from_sets([a, b], universe=int(max(a[-1], b[-1]))))
+    r = oracle.run_ref("stdintersection", path, threads=os.cpu_count())
+    return r["host_ms"]["std::set intersection"]
+
+
+def port_step_ms(a, b) -> float:
+    import oracle
+    t0 = time.perf_counter()
+    oracle.count(a, b, "std")
+    return (time.perf_counter() - t0) * 1e3
+
+
+def cpu_measure(a, b, steps: int, warmup: int):
+    import oracle
+    kind = "reference" if oracle.ref_binary("stdintersection") else "port"
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        for i in range(warmup + steps):
+            ms = reference_step_ms(a, b, td) if kind == "reference" else port_step_ms(a, b)
+            if i >= warmup:
+                times.append(ms)
+    return kind, times
+
+
+def run_reference_arm(args, rank: int):
+    if rank != 0:
+        return
+    # sized so that (steps + warmup) runs stay within a few minutes
+    per_step_budget = max(1 << 18, int((1 << 26) * 40 / max(1, args.steps + args.warmup)))
+    (a, b), desc = sample_pair(args.workload, per_step_budget)
+    kind, times = cpu_measure(a, b, args.steps, args.warmup)
+    ms = statistics.median(times)
+    value = (a.size + b.size) / (ms * 1e-3) / 1e9
+    line = {
+        "impl": "reference", "metric": "SISI Gelem/s", "value": value, "unit": "Gelem/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "technique": "std::set_intersection"},
+        "cpu_baseline": {"value": value, "unit": "Gelem/s", "cores": 1, "kind": kind,
+                         "sample": desc + "; stdintersection --threads nproc: with 2 sets only one thread has work "
+                                          "(src/std_set_intersection.cpp:58-76); median of steps"},
+        "e2e": {"value": value, "unit": "Gelem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------------- ours --
+def run_ours(args, rank: int, world: int):
+    import torch
+    from set_intersection_b200 import api
+    from set_intersection_b200._lib import lib
+    import ctypes
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        dist.init_process_group("nccl", device_id=dev)
+
+    # inputs: rank 0 generates (or loads the cache), the others load the cache
+    if rank == 0:
+        a, b = make_pair(args.workload)
+    if dist:
+        dist.barrier()
+    if rank != 0:
+        a, b = make_pair(args.workload)
+
+    n_a, n_b = a.size, b.size
+    stream = torch.cuda.Stream(dev)
+    da = torch.from_numpy(a.view(np.int32)).to(dev)
+    db = torch.from_numpy(b.view(np.int32)).to(dev)
+    ws = api.Workspace(dev)
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    out = torch.empty(max(1, min(n_a, n_b)), dtype=torch.int32, device=dev) if args.materialize else None
+
+    # parity of the benchmarked call, once, before timing
+    api.sisi_into(da, db, count, out, ws, args.technique, stream)
+    ws.check(stream)
+    c = int(count.item())
+    parity = None
+    if rank == 0 and not args.no_parity:
+        import oracle
+        want = oracle.set_intersection(a, b)
+        parity = bool(want.size == c and (out is None or np.array_equal(out[:c].cpu().numpy().view(np.uint32), want)))
+        log(f"parity vs oracle: {parity} (count {c})")
+
+    def step():
+        api.sisi_into(da, db, count, out, ws, args.technique, stream)
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    lib.si_timer_reset()
+    lib.si_timer_enable(1)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        stop.record(stream)
+        stop.synchronize()
+    lib.si_timer_enable(0)
+    ms_total = start.elapsed_time(stop)
+    tile_ms, tile_n = ctypes.c_double(0), ctypes.c_uint64(0)
+    lib.si_timer_read(b"ip_tile", ctypes.byref(tile_ms), ctypes.byref(tile_n))
+    lib.si_timer_reset()
+    ws.check(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+
+    ms_step = ms_total / args.steps
+    value = world * (n_a + n_b) / (ms_step * 1e-3) / 1e9
+
+    # ---- end to end through the public host API ----
+    e2e = None
+    if not args.no_e2e:
+        ha = torch.from_numpy(a.view(np.int32)).pin_memory()
+        hb = torch.from_numpy(b.view(np.int32)).pin_memory()
+        hout = torch.empty(max(1, min(n_a, n_b)), dtype=torch.int32).pin_memory()
+        ctx = api.HostPair(dev)
+        for _ in range(2):
+            api.intersect_host(ha, hb, args.technique, hout, ctx, stream)
+        e_steps = max(1, min(args.steps, args.e2e_steps))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e_steps):
+            ce, _ = api.intersect_host(ha, hb, args.technique, hout, ctx, stream)
+        e1.record(stream)
+        e1.synchronize()
+        e_ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e_step = e_ms / e_steps
+        e2e = {"value": world * (n_a + n_b) / (e_step * 1e-3) / 1e9, "unit": "Gelem/s",
+               "h2d_bytes_per_step": 4 * (n_a + n_b), "d2h_bytes_per_step": 8 + 4 * ce,
+               "ms_per_step": e_step, "steps": e_steps}
+        assert ce == c
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel ----
+    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    alg_bytes = 4 * (n_a + n_b) + (4 * c if args.materialize else 0)
+    tile_avg_ms = tile_ms.value / max(1, tile_n.value)
+    achieved = alg_bytes / (tile_avg_ms * 1e-3) / 1e9 if tile_n.value else None
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(f"ip_tile/{args.workload}/{'out' if args.materialize else 'count'}")
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        (sa, sb), desc = sample_pair(args.workload, 1 << 26)
+        kind, times = cpu_measure(sa, sb, steps=3, warmup=1)
+        cms = statistics.median(times)
+        cpu = {"value": (sa.size + sb.size) / (cms * 1e-3) / 1e9, "unit": "Gelem/s", "cores": 1, "kind": kind,
+               "sample": desc + "; median of 3 runs of the reference's stdintersection (one pair: one thread "
+                                "has work, src/std_set_intersection.cpp:58-76), timed by its HostTimer"}
+
+    line = {
+        "metric": "SISI Gelem/s", "value": value, "unit": "Gelem/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
+                   "technique": args.technique, "materialize": bool(args.materialize),
+                   "n_a": int(n_a), "n_b": int(n_b), "intersection": c,
+                   "l2": "inputs 2 GiB per step > 126 MB L2; no flush" if args.workload == "sisi_large"
+                         else "inputs resident; no flush",
+                   "parallelism": f"replicas{world}", "parity_vs_oracle": parity},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "kernel": "ip_tile_kernel", "alg_bytes_per_launch": alg_bytes,
+                     "avg_launch_ms": tile_avg_ms, "launches": int(tile_n.value), "peak_source": peak_src},
+        "e2e": e2e,
+        "gpu_launches": 3 * args.steps,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=sorted(WORKLOADS), default="sisi_large")
+    p.add_argument("--technique", default="ip")
+    p.add_argument("--count-only", dest="materialize", action="store_false")
+    p.add_argument("--e2e-steps", type=int, default=10)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-parity", action="store_true")
+    args = p.parse_args()
+    if args.warmup < 3:
+        p.error("--warmup must be >= 3")
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+    else:
+        run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,120 @@
+/*
+ * si.h -- C ABI of the B200 set-intersection engine (libsi_b200.so).
+ *
+ * The reference (chribell/set_intersection) exposes no library: each technique
+ * is a standalone executable whose hot path is a host loop that launches
+ * sm_61 kernels on a dataset already copied to the device.  Each entry point
+ * below replaces one such hot path and is what a per-technique executable (or
+ * any other host code) calls instead of the reference's kernels; the cited
+ * file:line ranges are the reference code each one replaces.
+ *
+ * Conventions
+ *  - All set pointers are DEVICE pointers to ascending, duplicate-free uint32
+ *    arrays (the reference assumes this and never checks it; si_validate_sorted
+ *    checks it on the device).  They must be 4-byte aligned.
+ *  - Everything is stream-ordered on the given stream (NULL = legacy default
+ *    stream) and asynchronous; nothing synchronises unless documented.
+ *  - The library never allocates device memory on these paths: scratch comes
+ *    from the caller as a workspace of the size the matching *_workspace_size
+ *    function returns.  It never calls exit().
+ *  - Device-detected problems (unsorted input, a bounded wait that gave up,
+ *    output overflow) are recorded in the workspace's error word;
+ *    si_workspace_check reads it back.
+ *  - Counts of one pair are uint32 as in the reference, except the single-pair
+ *    (SISI) count, which is uint64.
+ */
+#ifndef SI_B200_H
+#define SI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same handle as cudaStream_t. */
+typedef struct CUstream_st* si_stream_t;
+
+typedef enum si_status {
+    SI_OK = 0,
+    SI_ERR_INVALID_ARGUMENT = 1,   /* bad pointer, size or enum value (host-side check) */
+    SI_ERR_WORKSPACE_TOO_SMALL = 2,
+    SI_ERR_CUDA = 3,               /* a CUDA runtime call failed; see si_last_error_string */
+    SI_ERR_UNSUPPORTED = 4,        /* technique not available for this entry point */
+    SI_ERR_TIMEOUT = 5,            /* a bounded device-side wait gave up (device error word) */
+    SI_ERR_INVALID_INPUT = 6,      /* a set is not strictly increasing (device error word) */
+    SI_ERR_OUTPUT_OVERFLOW = 7     /* materialised output exceeded out_cap (device error word) */
+} si_status;
+
+/* Techniques: one per reference executable (CMakeLists.txt:56-160). */
+typedef enum si_technique {
+    SI_TECH_IP = 0,            /* intersect-path merge partitioning      (src/ip.cu) */
+    SI_TECH_OBS = 1,           /* optimized binary search, cached tree   (src/obs.cu) */
+    SI_TECH_HI = 2,            /* hash intersection                      (src/hi.cu) */
+    SI_TECH_BITMAP = 3,        /* dynamic bitmap probe                   (src/bitmap_dynamic.cu) */
+    SI_TECH_BITMAP_NAIVE = 4,  /* all-set bitmaps, plain AND-popcount    (src/bitmap_naive.cu) */
+    SI_TECH_MM = 5,            /* incidence-matrix product               (src/matrix_multiplication.cu) */
+    SI_TECH_AUTO = 6           /* the engine picks per input */
+} si_technique;
+
+const char* si_version(void);
+const char* si_status_string(si_status s);
+/* Text of the last CUDA error seen by this thread (empty if none). */
+const char* si_last_error_string(void);
+
+/* ------------------------------------------------------------------ SISI --
+ * One pair: count |A ∩ B| and optionally write the sorted elements of A ∩ B.
+ *
+ * Replaces the single-instance path of the GPU executables: src/ip.cu:141-177
+ * (findDiagonals + intersectPath for the one pair of a 2-set file),
+ * src/obs.cu:180-229 and src/hi.cu:205-245 with --path (intersectPathOBS,
+ * intersectPathHI), src/bitmap_dynamic.cu:168-176 (constructBitmap +
+ * singleInstanceIntersect + thrust::reduce).  The reference writes only the
+ * count; element output is this engine's addition, ordered as
+ * std::set_intersection orders it.
+ *
+ * d_count: device uint64, receives |A ∩ B|.
+ * d_out:   device uint32[out_cap] or NULL (count only).  When non-NULL,
+ *          out_cap must be >= min(nA, nB).
+ */
+size_t si_sisi_workspace_size(uint64_t nA, uint64_t nB, si_technique t);
+si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB,
+                  si_technique t, uint64_t* d_count, uint32_t* d_out, uint64_t out_cap,
+                  void* d_workspace, size_t workspace_bytes, si_stream_t stream);
+
+/* Synchronises the stream and returns the error recorded in a workspace by the
+ * last call that used it (SI_OK if none). */
+si_status si_workspace_check(const void* d_workspace, si_stream_t stream);
+
+/* Device-side check that x[0..n) is strictly increasing.  Writes 1 (ok) or 0
+ * to d_flag (device uint32).  No workspace. */
+si_status si_validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, si_stream_t stream);
+
+/* ---------------------------------------------------------- phase timer --
+ * Named cudaEvent pairs around the engine's own kernel launches, recorded on
+ * the launching stream while enabled -- the counterpart of the reference's
+ * DeviceTimer (include/device_timer.cuh:20-78), which wraps every phase of
+ * every executable the same way.  Phase names: "ip_prepare", "ip_split",
+ * "ip_tile".  si_timer_read synchronises on the recorded events and returns
+ * the summed milliseconds and the number of launches of one phase.
+ */
+void si_timer_enable(int on);
+void si_timer_reset(void);
+si_status si_timer_read(const char* phase, double* total_ms, uint64_t* launches);
+
+/* ------------------------------------------------------- data generators --
+ * Seeded, deterministic host generators for the benchmark configurations
+ * (stand-in for src/generate_dataset.cpp, whose std::random_device seed is not
+ * reproducible).  threads <= 0 uses all cores.
+ *
+ * si_gen_uniform: n distinct values drawn uniformly without replacement from
+ * [lo, hi), written ascending to out[n].  hi - lo <= 2^32.
+ */
+si_status si_gen_uniform(uint64_t seed, uint64_t n, uint64_t lo, uint64_t hi, uint32_t* out, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SI_B200_H */

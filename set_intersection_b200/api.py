@@ -1,0 +1,167 @@
+"""PyTorch-facing wrappers over the C ABI (torch supplies device memory and
+streams; all compute is in libsi_b200.so).
+
+Sets are 1-D contiguous CUDA tensors of dtype int32 or uint32 holding the
+uint32 bit patterns of an ascending, duplicate-free set.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from ._lib import Status, Technique, check, lib
+
+_TECH_NAMES = {
+    "ip": Technique.IP,
+    "obs": Technique.OBS,
+    "hi": Technique.HI,
+    "bitmap": Technique.BITMAP,
+    "bitmap_dynamic": Technique.BITMAP,
+    "bitmap_naive": Technique.BITMAP_NAIVE,
+    "mm": Technique.MM,
+    "auto": Technique.AUTO,
+}
+
+
+def technique(t) -> Technique:
+    if isinstance(t, Technique):
+        return t
+    if isinstance(t, int):
+        return Technique(t)
+    try:
+        return _TECH_NAMES[str(t).lower()]
+    except KeyError as e:
+        raise ValueError(f"unknown technique {t!r}; one of {sorted(_TECH_NAMES)}") from e
+
+
+def _ptr(t: torch.Tensor | None) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr() if t is not None and t.numel() > 0 else None)
+
+
+def _stream(stream: torch.cuda.Stream | None) -> ctypes.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _check_set(x: torch.Tensor, name: str) -> None:
+    if x.dim() != 1 or not x.is_cuda or not x.is_contiguous():
+        raise ValueError(f"{name} must be a 1-D contiguous CUDA tensor")
+    if x.dtype not in (torch.int32, torch.uint32):
+        raise ValueError(f"{name} must hold uint32 bit patterns (int32 or uint32 dtype)")
+
+
+class Workspace:
+    """Grow-only device scratch buffer reused across calls on one stream."""
+
+    def __init__(self, device=None):
+        self.device = torch.device(device if device is not None else "cuda")
+        self.buf = torch.empty(0, dtype=torch.uint8, device=self.device)
+
+    def get(self, nbytes: int) -> torch.Tensor:
+        nbytes = max(int(nbytes), 256)
+        if self.buf.numel() < nbytes:
+            self.buf = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        return self.buf
+
+    def check(self, stream=None) -> None:
+        """Synchronises and raises if the last call recorded a device error."""
+        check(lib.si_workspace_check(_ptr(self.buf), _stream(stream)), "device")
+
+
+def sisi_workspace_size(n_a: int, n_b: int, tech="ip") -> int:
+    return int(lib.si_sisi_workspace_size(n_a, n_b, int(technique(tech))))
+
+
+def sisi_into(a: torch.Tensor, b: torch.Tensor, count: torch.Tensor, out: torch.Tensor | None,
+              workspace: Workspace, tech="ip", stream=None) -> None:
+    """Asynchronous single-pair call: count (int64[1]) <- |a ∩ b|, out[:count]
+    <- the sorted intersection when out is given (len(out) >= min(|a|, |b|))."""
+    _check_set(a, "a")
+    _check_set(b, "b")
+    t = technique(tech)
+    n_a, n_b = a.numel(), b.numel()
+    ws = workspace.get(lib.si_sisi_workspace_size(n_a, n_b, int(t)))
+    cap = out.numel() if out is not None else 0
+    st = lib.si_sisi(_ptr(a), n_a, _ptr(b), n_b, int(t), _ptr(count),
+                     _ptr(out) if out is not None else ctypes.c_void_p(None), cap,
+                     _ptr(ws), ws.numel(), _stream(stream))
+    check(st, "si_sisi")
+
+
+def intersect(a: torch.Tensor, b: torch.Tensor, tech="ip", materialize: bool = True,
+              workspace: Workspace | None = None, stream=None):
+    """|a ∩ b| and (if materialize) the sorted elements, synchronously.
+
+    Returns (count: int, elements: int32 CUDA tensor or None)."""
+    ws = workspace or Workspace(a.device)
+    count = torch.zeros(1, dtype=torch.int64, device=a.device)
+    out = None
+    if materialize:
+        out = torch.empty(max(1, min(a.numel(), b.numel())), dtype=torch.int32, device=a.device)
+    sisi_into(a, b, count, out, ws, tech, stream)
+    ws.check(stream)
+    c = int(count.item())
+    return c, (out[:c] if out is not None else None)
+
+
+class HostPair:
+    """Device buffers and workspace reused by intersect_host across calls."""
+
+    def __init__(self, device=None):
+        self.device = torch.device(device if device is not None else "cuda")
+        self.ws = Workspace(self.device)
+        self.dev_a = self.dev_b = self.dev_out = None
+        self.count = torch.zeros(1, dtype=torch.int64, device=self.device)
+        self.count_host = torch.zeros(1, dtype=torch.int64).pin_memory()
+
+    def _fit(self, buf, n):
+        if buf is None or buf.numel() < n:
+            buf = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        return buf
+
+
+def intersect_host(a_host: torch.Tensor, b_host: torch.Tensor, tech="ip", out_host: torch.Tensor | None = None,
+                   ctx: HostPair | None = None, stream=None):
+    """End-to-end single pair from HOST sets: copies a and b to the device,
+    intersects, and copies the count and the sorted elements back.
+
+    a_host/b_host: 1-D int32/uint32 CPU tensors (pinned for asynchronous
+    copies).  out_host: optional pinned int32 buffer of >= min(|a|, |b|)
+    elements that receives the result.  Returns (count, host tensor view)."""
+    ctx = ctx or HostPair()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    n_a, n_b = a_host.numel(), b_host.numel()
+    ctx.dev_a = ctx._fit(ctx.dev_a, n_a)
+    ctx.dev_b = ctx._fit(ctx.dev_b, n_b)
+    ctx.dev_out = ctx._fit(ctx.dev_out, min(n_a, n_b))
+    da, db = ctx.dev_a[:n_a], ctx.dev_b[:n_b]
+    with torch.cuda.stream(s):
+        da.copy_(a_host.view(torch.int32), non_blocking=True)
+        db.copy_(b_host.view(torch.int32), non_blocking=True)
+        sisi_into(da, db, ctx.count, ctx.dev_out, ctx.ws, tech, s)
+        ctx.count_host.copy_(ctx.count, non_blocking=True)
+    s.synchronize()
+    c = int(ctx.count_host[0])
+    if out_host is None:
+        out_host = torch.empty(max(c, 1), dtype=torch.int32).pin_memory()
+    with torch.cuda.stream(s):
+        out_host[:c].copy_(ctx.dev_out[:c], non_blocking=True)
+    s.synchronize()
+    return c, out_host[:c]
+
+
+def validate_sorted(x: torch.Tensor, stream=None) -> bool:
+    _check_set(x, "x")
+    flag = torch.zeros(1, dtype=torch.int32, device=x.device)
+    check(lib.si_validate_sorted(_ptr(x), x.numel(), _ptr(flag), _stream(stream)), "si_validate_sorted")
+    return bool(flag.item())
+
+
+def status_string(s: int) -> str:
+    return lib.si_status_string(int(s)).decode()
+
+
+__all__ = ["Status", "Technique", "Workspace", "HostPair", "intersect", "intersect_host", "sisi_into",
+           "sisi_workspace_size",
+           "technique", "validate_sorted", "status_string"]

@@ -1,0 +1,202 @@
+// si_api.cu -- the C ABI of libsi_b200.so: argument checks, technique
+// dispatch, workspace sizing, error reporting.  Declarations and the
+// reference interfaces each entry point replaces are in include/si.h.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "si_device.cuh"
+#include "si_internal.h"
+
+namespace si {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+si_status cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return SI_ERR_CUDA;
+}
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (cached[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cached[dev] = n;
+    }
+    return cached[dev];
+}
+
+namespace {
+
+struct TimerRecord {
+    std::string name;
+    cudaEvent_t start = nullptr, stop = nullptr;
+};
+std::mutex g_timer_mu;
+bool g_timer_on = false;
+std::vector<TimerRecord> g_timer;
+
+}  // namespace
+
+PhaseTimer::PhaseTimer(const char* name, cudaStream_t stream) : slot_(-1), stream_(stream) {
+    std::lock_guard<std::mutex> lk(g_timer_mu);
+    if (!g_timer_on) return;
+    TimerRecord r;
+    r.name = name;
+    if (cudaEventCreate(&r.start) != cudaSuccess) return;
+    if (cudaEventCreate(&r.stop) != cudaSuccess) {
+        cudaEventDestroy(r.start);
+        return;
+    }
+    cudaEventRecord(r.start, stream);
+    g_timer.push_back(r);
+    slot_ = static_cast<int>(g_timer.size()) - 1;
+}
+
+PhaseTimer::~PhaseTimer() {
+    if (slot_ < 0) return;
+    std::lock_guard<std::mutex> lk(g_timer_mu);
+    if (slot_ < static_cast<int>(g_timer.size())) cudaEventRecord(g_timer[slot_].stop, stream_);
+}
+
+namespace {
+
+void timer_clear_locked() {
+    for (auto& r : g_timer) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    g_timer.clear();
+}
+
+// flag starts at 1; any descending-or-equal adjacent pair clears it.
+__global__ void validate_sorted_kernel(const uint32_t* __restrict__ x, uint64_t n, uint32_t* flag) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    bool bad = false;
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x + 1; k < n; k += stride)
+        bad |= __ldg(x + k - 1) >= __ldg(x + k);
+    if (__any_sync(kFullMask, bad) && (threadIdx.x & 31) == 0) atomicExch(flag, 0u);
+}
+
+__global__ void set_flag_kernel(uint32_t* flag, uint32_t v) { *flag = v; }
+
+bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+}  // namespace
+
+si_status validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, cudaStream_t stream) {
+    set_flag_kernel<<<1, 1, 0, stream>>>(d_flag, 1u);
+    SI_LAUNCH_CHECK("set_flag_kernel");
+    if (n > 1) {
+        const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, static_cast<uint64_t>(sm_count()) * 8);
+        validate_sorted_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(d_x, n, d_flag);
+        SI_LAUNCH_CHECK("validate_sorted_kernel");
+    }
+    return SI_OK;
+}
+
+}  // namespace si
+
+extern "C" {
+
+const char* si_version(void) { return "set_intersection_b200 0.1.0 (sm_100a)"; }
+
+const char* si_status_string(si_status s) {
+    switch (s) {
+        case SI_OK: return "ok";
+        case SI_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case SI_ERR_WORKSPACE_TOO_SMALL: return "workspace too small";
+        case SI_ERR_CUDA: return "CUDA error";
+        case SI_ERR_UNSUPPORTED: return "unsupported technique for this entry point";
+        case SI_ERR_TIMEOUT: return "a bounded device-side wait gave up";
+        case SI_ERR_INVALID_INPUT: return "input set is not strictly increasing";
+        case SI_ERR_OUTPUT_OVERFLOW: return "materialised output exceeded its capacity";
+    }
+    return "unknown status";
+}
+
+const char* si_last_error_string(void) { return si::g_last_error.c_str(); }
+
+size_t si_sisi_workspace_size(uint64_t nA, uint64_t nB, si_technique t) {
+    switch (t) {
+        case SI_TECH_IP:
+        case SI_TECH_AUTO:
+            return si::ip_workspace_size(nA, nB);
+        default:
+            return 0;
+    }
+}
+
+si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, si_technique t,
+                  uint64_t* d_count, uint32_t* d_out, uint64_t out_cap, void* d_workspace, size_t workspace_bytes,
+                  si_stream_t stream) {
+    if ((nA && !dA) || (nB && !dB) || !d_count || !d_workspace) return SI_ERR_INVALID_ARGUMENT;
+    if (!si::aligned(dA, 4) || !si::aligned(dB, 4) || !si::aligned(d_count, 8) || !si::aligned(d_workspace, 16) ||
+        (d_out && !si::aligned(d_out, 4)))
+        return SI_ERR_INVALID_ARGUMENT;
+    if (d_out && out_cap < (nA < nB ? nA : nB)) return SI_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    switch (t) {
+        case SI_TECH_IP:
+        case SI_TECH_AUTO:
+            return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, d_workspace, workspace_bytes, s);
+        case SI_TECH_OBS:
+        case SI_TECH_HI:
+        case SI_TECH_BITMAP:
+            return SI_ERR_UNSUPPORTED;
+        default:
+            return SI_ERR_INVALID_ARGUMENT;
+    }
+}
+
+si_status si_workspace_check(const void* d_workspace, si_stream_t stream) {
+    if (!d_workspace) return SI_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t code = 0;
+    SI_CUDA_TRY(cudaMemcpyAsync(&code, d_workspace, sizeof(code), cudaMemcpyDeviceToHost, s));
+    SI_CUDA_TRY(cudaStreamSynchronize(s));
+    return static_cast<si_status>(code);
+}
+
+void si_timer_enable(int on) {
+    std::lock_guard<std::mutex> lk(si::g_timer_mu);
+    si::g_timer_on = on != 0;
+}
+
+void si_timer_reset(void) {
+    std::lock_guard<std::mutex> lk(si::g_timer_mu);
+    si::timer_clear_locked();
+}
+
+si_status si_timer_read(const char* phase, double* total_ms, uint64_t* launches) {
+    if (!phase || !total_ms || !launches) return SI_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(si::g_timer_mu);
+    double sum = 0.0;
+    uint64_t n = 0;
+    for (auto& r : si::g_timer) {
+        if (r.name != phase) continue;
+        SI_CUDA_TRY(cudaEventSynchronize(r.stop));
+        float ms = 0.f;
+        SI_CUDA_TRY(cudaEventElapsedTime(&ms, r.start, r.stop));
+        sum += ms;
+        ++n;
+    }
+    *total_ms = sum;
+    *launches = n;
+    return SI_OK;
+}
+
+si_status si_validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, si_stream_t stream) {
+    if ((n && !d_x) || !d_flag || !si::aligned(d_x, 4) || !si::aligned(d_flag, 4)) return SI_ERR_INVALID_ARGUMENT;
+    return si::validate_sorted(d_x, n, d_flag, reinterpret_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+// si_device.cuh -- device-side building blocks shared by the sm_100a kernels:
+// mbarrier + 1-D bulk-copy (TMA) staging, release/acquire flags, warp scans and
+// the workspace error word.  Every wait here is bounded.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "si.h"
+
+namespace si {
+
+constexpr uint32_t kFullMask = 0xffffffffu;
+// Upper bound on polling iterations of any device-side wait before it gives up
+// and records SI_ERR_TIMEOUT.  With the back-off below this is well over a
+// second of wall time, far beyond any legitimate wait.
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+// ---------------------------------------------------------------- errors --
+// The first word of every workspace is the error word: 0 = ok, else si_status.
+__device__ __forceinline__ void record_error(uint32_t* err, si_status code) {
+    atomicCAS(err, 0u, static_cast<uint32_t>(code));
+}
+
+// --------------------------------------------------------------- smem/PTX --
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Makes an mbarrier initialisation visible to the async (TMA) proxy.
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait on an mbarrier phase; records SI_ERR_TIMEOUT and returns false
+// if it gives up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err) {
+    for (uint32_t spins = 0; spins < kSpinLimit; ++spins) {
+        if (mbar_try_wait(bar, parity)) return true;
+    }
+    record_error(err, SI_ERR_TIMEOUT);
+    return false;
+}
+
+// 1-D bulk copy global -> shared (TMA engine), completion counted on `bar`.
+// dst and src must be 16-byte aligned and bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// ------------------------------------------------------- flags (look-back) --
+__device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// ------------------------------------------------------------ warp scans --
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t n = __shfl_up_sync(kFullMask, v, d);
+        if (lane >= d) v += n;
+    }
+    return v;
+}
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kFullMask, v, d);
+    return v;
+}
+
+// ------------------------------------------------------ staging planning --
+// Plan for copying n uint32 from global g into a 16-byte aligned shared
+// buffer `buf` (capacity >= n + 8) so that element x lands at dst[x]:
+// the 16-byte aligned middle goes through the bulk-copy engine, the <= 3
+// leading and <= 3 trailing elements through ordinary loads.
+struct StagePlan {
+    uint32_t* dst;   // shared address of element 0
+    int head;        // elements [0, head) by plain loads
+    int body;        // elements [head, head + body) by bulk copy (body % 4 == 0)
+    int n;           // elements [head + body, n) by plain loads
+};
+
+__device__ __forceinline__ StagePlan plan_stage(const uint32_t* g, int n, uint32_t* buf) {
+    StagePlan p;
+    const int mis = static_cast<int>((reinterpret_cast<uintptr_t>(g) & 15u) >> 2);
+    int head = mis ? 4 - mis : 0;
+    if (head > n) head = n;
+    p.head = head;
+    p.body = ((n - head) >> 2) << 2;
+    p.dst = buf + ((4 - head) & 3);
+    p.n = n;
+    return p;
+}
+
+// Issued by one thread: the bulk part of a plan.
+__device__ __forceinline__ void issue_stage(const StagePlan& p, const uint32_t* g, uint64_t* bar) {
+    if (p.body > 0) bulk_g2s(p.dst + p.head, g + p.head, static_cast<uint32_t>(p.body) * 4u, bar);
+}
+
+// Done by threads [0, 6): the plain-load edges of a plan.
+__device__ __forceinline__ void edge_stage(const StagePlan& p, const uint32_t* g, int slot) {
+    int x = slot < 3 ? slot : p.head + p.body + (slot - 3);
+    bool want = slot < 3 ? (slot < p.head) : (x < p.n);
+    if (want) p.dst[x] = __ldg(g + x);
+}
+
+}  // namespace si

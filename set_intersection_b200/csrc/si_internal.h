@@ -1,0 +1,55 @@
+// si_internal.h -- host-side interfaces between the C-ABI layer (si_api.cu)
+// and the per-technique launchers.  Not installed; C++ only.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "si.h"
+
+namespace si {
+
+// Records a CUDA error text for si_last_error_string and returns SI_ERR_CUDA.
+si_status cuda_fail(cudaError_t e, const char* what);
+
+#define SI_CUDA_TRY(expr)                                                 \
+    do {                                                                  \
+        cudaError_t si_e_ = (expr);                                       \
+        if (si_e_ != cudaSuccess) return ::si::cuda_fail(si_e_, #expr);   \
+    } while (0)
+
+#define SI_LAUNCH_CHECK(what)                                             \
+    do {                                                                  \
+        cudaError_t si_e_ = cudaGetLastError();                           \
+        if (si_e_ != cudaSuccess) return ::si::cuda_fail(si_e_, what);    \
+    } while (0)
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+// Named phase timing on the launching stream (the engine's counterpart of the
+// reference's DeviceTimer, include/device_timer.cuh:20-78).  When enabled via
+// si_timer_enable, PhaseTimer records a cudaEvent pair around a launch.
+class PhaseTimer {
+public:
+    PhaseTimer(const char* name, cudaStream_t stream);
+    ~PhaseTimer();
+    PhaseTimer(const PhaseTimer&) = delete;
+    PhaseTimer& operator=(const PhaseTimer&) = delete;
+private:
+    int slot_;
+    cudaStream_t stream_;
+};
+
+// ---- intersect-path SISI (si_sisi_ip.cu) ----
+size_t ip_workspace_size(uint64_t nA, uint64_t nB);
+si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
+                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream);
+
+// ---- sortedness check (si_api.cu) ----
+si_status validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, cudaStream_t stream);
+
+}  // namespace si

@@ -1,0 +1,54 @@
+"""Seeded synthetic inputs for the benchmark configurations (host-side).
+
+The reference's generator (src/generate_dataset.cpp) seeds from
+std::random_device, so its datasets cannot be reproduced; these generators are
+deterministic given a seed and run in the library's C++ host code
+(si_gen_uniform) or numpy.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import check, lib
+
+
+def uniform(seed: int, n: int, hi: int, lo: int = 0, threads: int = 0) -> np.ndarray:
+    """n distinct uint32 drawn uniformly without replacement from [lo, hi), ascending."""
+    out = np.empty(n, dtype=np.uint32)
+    st = lib.si_gen_uniform(seed, n, lo, hi, out.ctypes.data_as(ctypes.c_void_p), threads)
+    check(st, "si_gen_uniform")
+    return out
+
+
+def sisi_plain(seed_a: int = 1, seed_b: int = 2, n: int = 1 << 20, universe: int = 1 << 24):
+    """|A| = |B| = 2^20 from [0, 2^24), seeds 1 and 2 (the plain single-pair case)."""
+    return uniform(seed_a, n, universe), uniform(seed_b, n, universe)
+
+
+def sisi_large(seed_a: int = 3, seed_b: int = 4, n: int = 1 << 28, universe: int = 1 << 31):
+    """|A| = |B| = 2^28 from [0, 2^31) (the large single-pair case)."""
+    return uniform(seed_a, n, universe), uniform(seed_b, n, universe)
+
+
+def sisi_skewed(seed: int = 5, n_small: int = 1 << 16, n_large: int = 1 << 26,
+                universe: int = 1 << 30, planted_frac: float = 0.2):
+    """|A| = 2^16, |B| = 2^26 from [0, 2^30), with round(0.2*|A|) elements of A
+    planted into B.  B's other elements are uniform over the universe minus the
+    planted values (rank mapping), so |B| is exact."""
+    a = uniform(seed, n_small, universe)
+    n_plant = int(round(planted_frac * n_small))
+    pick = uniform(seed + 1000003, n_plant, n_small)          # indices into a
+    planted = a[pick.astype(np.int64)]
+    w = uniform(seed + 2000003, n_large - n_plant, universe - n_plant).astype(np.int64)
+    # map w in [0, U - P) to the w-th value of [0, U) that is not planted
+    q = planted.astype(np.int64) - np.arange(n_plant, dtype=np.int64)
+    rest = w + np.searchsorted(q, w, side="right")
+    b = np.empty(n_large, dtype=np.uint32)
+    pos_p = np.searchsorted(rest, planted.astype(np.int64)) + np.arange(n_plant)
+    mask = np.ones(n_large, dtype=bool)
+    mask[pos_p] = False
+    b[pos_p] = planted
+    b[mask] = rest.astype(np.uint32)
+    return a, b

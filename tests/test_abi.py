@@ -1,0 +1,96 @@
+"""The C-ABI library loads and exports what include/si.h declares; host-side
+argument checks and host generators work without a GPU."""
+import ctypes
+import subprocess
+
+import numpy as np
+import pytest
+
+import set_intersection_b200 as si
+from set_intersection_b200 import _lib
+from set_intersection_b200._lib import Status, Technique
+
+
+def test_every_declared_symbol_is_exported():
+    declared = si.declared_symbols()
+    assert "si_sisi" in declared
+    out = subprocess.run(["nm", "-D", "--defined-only", si.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [s for s in declared if s not in exported]
+    assert not missing, f"declared in include/si.h but not exported: {missing}"
+    for s in declared:
+        assert getattr(si.lib, s) is not None
+
+
+def test_exports_are_plain_c_symbols():
+    out = subprocess.run(["nm", "-D", "--defined-only", si.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    names = [line.split()[-1] for line in out.splitlines() if " T " in line]
+    si_names = [n for n in names if n.startswith("si_")]
+    assert si_names and all("_Z" not in n for n in si_names)
+
+
+def test_version_and_status_strings():
+    assert b"sm_100a" in si.lib.si_version()
+    for s in Status:
+        assert si.lib.si_status_string(int(s))
+    assert si.lib.si_status_string(99) == b"unknown status"
+
+
+def test_invalid_arguments_rejected_on_host():
+    L = si.lib
+    nul = ctypes.c_void_p(None)
+    fake = ctypes.c_void_p(0x1000)
+    # null count / workspace
+    assert L.si_sisi(fake, 4, fake, 4, int(Technique.IP), nul, nul, 0, fake, 1 << 20, nul) == Status.INVALID_ARGUMENT
+    assert L.si_sisi(fake, 4, fake, 4, int(Technique.IP), fake, nul, 0, nul, 1 << 20, nul) == Status.INVALID_ARGUMENT
+    # misaligned set pointer
+    assert L.si_sisi(ctypes.c_void_p(0x1002), 4, fake, 4, int(Technique.IP), fake, nul, 0, fake, 1 << 20,
+                     nul) == Status.INVALID_ARGUMENT
+    # output capacity below min(nA, nB)
+    assert L.si_sisi(fake, 40, fake, 50, int(Technique.IP), fake, fake, 39, fake, 1 << 20,
+                     nul) == Status.INVALID_ARGUMENT
+    # workspace too small is detected before any launch
+    assert L.si_sisi(fake, 1 << 20, fake, 1 << 20, int(Technique.IP), fake, nul, 0, fake, 64,
+                     nul) == Status.WORKSPACE_TOO_SMALL
+    # unknown technique
+    assert L.si_sisi(fake, 4, fake, 4, 42, fake, nul, 0, fake, 1 << 20, nul) == Status.INVALID_ARGUMENT
+    assert L.si_validate_sorted(fake, 4, nul, nul) == Status.INVALID_ARGUMENT
+    assert L.si_workspace_check(nul, nul) == Status.INVALID_ARGUMENT
+
+
+def test_workspace_size_grows_with_input():
+    f = si.lib.si_sisi_workspace_size
+    small = f(1000, 1000, int(Technique.IP))
+    big = f(1 << 28, 1 << 28, int(Technique.IP))
+    assert 0 < small < big
+    # scratch is a small fraction of the input it partitions
+    assert big < (2 << 28) * 4 // 100
+
+
+def test_uniform_generator_is_exact_and_deterministic():
+    from set_intersection_b200 import generate as g
+    for n, hi in ((1000, 1 << 12), (5000, 1 << 30), (1 << 16, 1 << 18)):
+        x = g.uniform(11, n, hi)
+        assert x.size == n and x.dtype == np.uint32
+        assert np.all(x[1:] > x[:-1]) and int(x[-1]) < hi
+        np.testing.assert_array_equal(x, g.uniform(11, n, hi, threads=3))
+        assert not np.array_equal(x, g.uniform(12, n, hi))
+    full = g.uniform(1, 4096, 4096)
+    np.testing.assert_array_equal(full, np.arange(4096, dtype=np.uint32))
+
+
+def test_uniform_generator_rejects_bad_ranges():
+    from set_intersection_b200 import generate as g
+    with pytest.raises(_lib.SiError):
+        g.uniform(1, 10, 5)
+    with pytest.raises(_lib.SiError):
+        g.uniform(1, 1, (1 << 32) + 1)
+
+
+def test_skewed_generator_plants_overlap():
+    import oracle
+    from set_intersection_b200 import generate as g
+    a, b = g.sisi_skewed(seed=9, n_small=1 << 10, n_large=1 << 16, universe=1 << 24)
+    assert a.size == 1 << 10 and b.size == 1 << 16
+    assert np.all(b[1:] > b[:-1])
+    assert oracle.count(a, b) >= int(round(0.2 * a.size))

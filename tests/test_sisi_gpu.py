@@ -1,0 +1,164 @@
+"""Single-pair (SISI) parity on the GPU: every count and every materialised
+element bit-exact against the oracle / the reference's golden outputs."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden_path, read_golden_elements
+from set_intersection_b200 import dataset as fmt
+
+pytestmark = pytest.mark.gpu
+
+TECHS = ["ip"]
+
+
+def dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x, dtype=np.uint32).view(np.int32)).cuda()
+
+
+def run(a, b, tech="ip", materialize=True, ws=None):
+    from set_intersection_b200 import api
+    c, out = api.intersect(dev(a), dev(b), tech, materialize, workspace=ws)
+    return c, (out.cpu().numpy().view(np.uint32) if out is not None else None)
+
+
+def check(a, b, tech="ip"):
+    want = oracle.set_intersection(a, b)
+    c, got = run(a, b, tech)
+    assert c == want.size
+    np.testing.assert_array_equal(got, want)
+    c2, _ = run(a, b, tech, materialize=False)
+    assert c2 == want.size
+
+
+@pytest.mark.parametrize("tech", TECHS)
+@pytest.mark.parametrize("name", ["sisi_uniform", "sisi_skewed", "sisi_extremes", "misi_mixed", "misi_onebased"])
+def test_golden_pairs(cuda, tech, name):
+    ds = fmt.read_dataset(golden_path(f"{name}.bin"))
+    want = read_golden_elements(f"{name}.elements.bin")
+    c, got = run(ds.set(0), ds.set(1), tech)
+    assert c == want.size
+    np.testing.assert_array_equal(got, want)
+    # either argument order gives the same intersection
+    c, got = run(ds.set(1), ds.set(0), tech)
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_all_golden_pairs_of_mixed_dataset(cuda, tech):
+    """Every pair of the mixed golden dataset (empty, singleton, identical,
+    subset, disjoint, ragged sizes) against the reference's result file."""
+    ds = fmt.read_dataset(golden_path("misi_mixed.bin"))
+    expected = fmt.parse_result(golden_path("misi_mixed.std.txt"), ds.cardinality)
+    sets = ds.sets()
+    k = ds.cardinality
+    from set_intersection_b200 import tiling
+    for a in range(0, k, 3):
+        for b in range(a + 1, k, 2):
+            c, _ = run(sets[a], sets[b], tech, materialize=False)
+            assert c == int(expected[tiling.triangular_index(k, a, b)]), (a, b)
+
+
+def _u(rng, n, hi):
+    return np.sort(rng.choice(hi, size=n, replace=False)).astype(np.uint32)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+@pytest.mark.parametrize("na,nb,hi", [
+    (0, 0, 10), (0, 100, 1000), (100, 0, 1000), (1, 1, 2), (3, 5, 8),
+    (4095, 4097, 1 << 14), (4096, 4096, 8192), (4097, 12289, 1 << 15),
+    (10000, 10, 1 << 20), (10, 10000, 1 << 20), (123457, 98765, 1 << 18),
+    (1 << 17, 1 << 17, 1 << 18),
+])
+def test_random_sizes(cuda, tech, na, nb, hi):
+    rng = np.random.default_rng(na * 31 + nb)
+    check(_u(rng, na, hi), _u(rng, nb, hi), tech)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_identical_disjoint_subset(cuda, tech):
+    x = np.arange(0, 300000, 3, dtype=np.uint32)
+    check(x, x.copy(), tech)
+    check(x, x + 1, tech)
+    check(x, x[::7].copy(), tech)
+    check(np.arange(0, 50000, dtype=np.uint32), np.arange(50000, 90000, dtype=np.uint32), tech)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_value_extremes(cuda, tech):
+    top = np.arange(0xffffffff - 20000, 0xffffffff + 1, dtype=np.uint64).astype(np.uint32)
+    check(top, top[::2].copy(), tech)
+    check(top[1::2].copy(), top[::2].copy(), tech)
+    check(np.array([0, 0xffffffff], np.uint32), np.array([0xffffffff], np.uint32), tech)
+    rng = np.random.default_rng(5)
+    a = np.concatenate([[0], _u(rng, 50000, 1 << 32 - 1)[1:-1], [0xffffffff]]).astype(np.uint32)
+    a = np.unique(a)
+    b = np.unique(np.concatenate([[0, 0xffffffff], a[::5]])).astype(np.uint32)
+    check(a, b, tech)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_misaligned_device_pointers(cuda, tech):
+    """Sets that start at any 4-byte offset (views into larger buffers)."""
+    from set_intersection_b200 import api
+    rng = np.random.default_rng(8)
+    base_a = _u(rng, 40011, 1 << 17)
+    base_b = _u(rng, 40007, 1 << 17)
+    da, db = dev(base_a), dev(base_b)
+    for oa, ob in ((1, 0), (0, 3), (2, 1), (3, 3)):
+        want = oracle.set_intersection(base_a[oa:], base_b[ob:])
+        c, out = api.intersect(da[oa:], db[ob:], tech)
+        assert c == want.size
+        np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), want)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_workspace_reuse_across_sizes(cuda, tech):
+    from set_intersection_b200 import api
+    ws = api.Workspace()
+    rng = np.random.default_rng(12)
+    for n in (50000, 7, 200000, 0, 4096):
+        a, b = _u(rng, n, 1 << 19), _u(rng, n, 1 << 19)
+        want = oracle.set_intersection(a, b)
+        c, got = run(a, b, tech, ws=ws)
+        assert c == want.size
+        np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_plain_config_seeds_1_2(cuda, tech):
+    """|A| = |B| = 2^20 from [0, 2^24), seeds 1 and 2."""
+    from set_intersection_b200 import generate
+    a, b = generate.sisi_plain()
+    check(a, b, tech)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_2_24_against_oracle(cuda, tech):
+    from set_intersection_b200 import generate
+    a = generate.uniform(21, 1 << 24, 1 << 27)
+    b = generate.uniform(22, 1 << 24, 1 << 27)
+    check(a, b, tech)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("tech", TECHS)
+def test_full_size_2_28(cuda, tech):
+    """|A| = |B| = 2^28 from [0, 2^31): full-size result equals the oracle's,
+    element for element."""
+    from set_intersection_b200 import generate
+    a, b = generate.sisi_large()
+    want = oracle.set_intersection(a, b)
+    c, got = run(a, b, tech)
+    assert c == want.size
+    assert np.array_equal(got, want)
+
+
+def test_validate_sorted(cuda):
+    from set_intersection_b200 import api
+    assert api.validate_sorted(dev(np.arange(100000, dtype=np.uint32)))
+    x = np.arange(100000, dtype=np.uint32)
+    x[54321] = x[54320]
+    assert not api.validate_sorted(dev(x))
+    assert api.validate_sorted(dev(np.zeros(1, np.uint32)))
