@@ -46,6 +46,9 @@ CACHE_DIR = os.environ.get("SI_BENCH_CACHE", os.path.join(tempfile.gettempdir(),
 WORKLOADS = {
     "sisi_large": dict(desc="SISI |A|=|B|=2^28 uint32 uniform w/o replacement from [0,2^31), seeds 3,4",
                        n=1 << 28, universe=1 << 31, seeds=(3, 4)),
+    "sisi_mid": dict(desc="SISI |A|=|B|=2^25 uint32 uniform w/o replacement from [0,2^28), seeds 3,4 "
+                          "(same density as sisi_large, 256 MiB > L2; profiling size)",
+                     n=1 << 25, universe=1 << 28, seeds=(3, 4)),
     "sisi_plain": dict(desc="SISI |A|=|B|=2^20 uint32 uniform w/o replacement from [0,2^24), seeds 1,2",
                        n=1 << 20, universe=1 << 24, seeds=(1, 2)),
     "sisi_skewed": dict(desc="SISI |A|=2^16, |B|=2^26 from [0,2^30), 20% of A planted into B, seed 5",

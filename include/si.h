@@ -83,6 +83,28 @@ si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
                   si_technique t, uint64_t* d_count, uint32_t* d_out, uint64_t out_cap,
                   void* d_workspace, size_t workspace_bytes, si_stream_t stream);
 
+/* Single pair without any caller-provided scratch.  No counterpart in the
+ * reference (whose executables cudaMalloc everything themselves).
+ *
+ * For callers that cannot allocate device memory: FFI hosts (cgo, JNI, ctypes)
+ * that receive device buffers from another runtime and have no CUDA allocator
+ * of their own, engines whose memory manager already owns the whole HBM
+ * budget, and paths where cudaMalloc/cudaFree would synchronise the device.
+ * Same kernels and results as si_sisi with SI_TECH_IP; the caller passes only
+ * inputs and outputs, and the call allocates nothing.
+ *
+ * Scratch is a fixed 4 MiB array in device memory owned by the library (held
+ * by every GPU that loads it, until the process exits), enough for any pair
+ * with |A| + |B| <= 2^29 elements; larger pairs are rejected with
+ * SI_ERR_WORKSPACE_TOO_SMALL before anything is launched.  The first call on a
+ * device looks up the array's device address (issue it before any stream
+ * capture).  All calls share the array: calls that may overlap on the GPU
+ * (e.g. on unordered streams) race and must not be issued.  Device-detected
+ * input errors are not reported (there is no caller workspace to read);
+ * check inputs with si_validate_sorted. */
+si_status si_sisi_noalloc(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB,
+                          uint64_t* d_count, uint32_t* d_out, uint64_t out_cap, si_stream_t stream);
+
 /* Synchronises the stream and returns the error recorded in a workspace by the
  * last call that used it (SI_OK if none). */
 si_status si_workspace_check(const void* d_workspace, si_stream_t stream);

@@ -64,6 +64,7 @@ _SIGNATURES = {
     "si_last_error_string": (ctypes.c_char_p, []),
     "si_sisi_workspace_size": (_sz, [_u64, _u64, _int]),
     "si_sisi": (_int, [_vp, _u64, _vp, _u64, _int, _vp, _vp, _u64, _vp, _sz, _vp]),
+    "si_sisi_noalloc": (_int, [_vp, _u64, _vp, _u64, _vp, _vp, _u64, _vp]),
     "si_workspace_check": (_int, [_vp, _vp]),
     "si_validate_sorted": (_int, [_vp, _u64, _vp, _vp]),
     "si_gen_uniform": (_int, [_u64, _u64, _u64, _u64, _vp, _int]),
