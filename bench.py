@@ -13,7 +13,7 @@ Metric: Gelem/s = (|A| + |B|) / step time.
           in HBM; 2 GiB of input per step > 126 MB L2, so no L2 flush.
   e2e     the same metric through the public host API (api.intersect_host):
           pinned host sets -> H2D -> kernels -> count + elements D2H, per step.
-  roofline  live per-launch time of the dominant kernel (ip_tile) from the
+  roofline  live per-launch time of the dominant kernel (the tile kernel) from the
           library's phase timer over the timed region, against measured HBM.
   cpu_baseline  the reference's own CPU executable (oracle/_ref/stdintersection,
           built from the reference sources) on a bounded sample of the same
@@ -281,7 +281,7 @@ def run_ours(args, rank: int, world: int):
     lib.si_timer_enable(0)
     ms_total = start.elapsed_time(stop)
     tile_ms, tile_n = ctypes.c_double(0), ctypes.c_uint64(0)
-    lib.si_timer_read(b"ip_tile", ctypes.byref(tile_ms), ctypes.byref(tile_n))
+    lib.si_timer_read(b"sisi_tile", ctypes.byref(tile_ms), ctypes.byref(tile_n))
     lib.si_timer_reset()
     ws.check(stream)
     torch.cuda.synchronize()
@@ -339,7 +339,7 @@ def run_ours(args, rank: int, world: int):
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
-        traffic = json.load(open(tf)).get(f"ip_tile/{args.workload}/{'out' if args.materialize else 'count'}")
+        traffic = json.load(open(tf)).get(f"{args.technique}/{args.workload}/{'out' if args.materialize else 'count'}")
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -362,7 +362,7 @@ def run_ours(args, rank: int, world: int):
                    "parallelism": f"replicas{world}", "parity_vs_oracle": parity},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "ip_tile_kernel", "alg_bytes_per_launch": alg_bytes,
+                     "kernel": f"ip_tile_kernel<{'bitmap probe' if args.technique in ('bitmap', 'auto') else 'merge path'}>", "alg_bytes_per_launch": alg_bytes,
                      "avg_launch_ms": tile_avg_ms, "launches": int(tile_n.value), "peak_source": peak_src},
         "e2e": e2e,
         "gpu_launches": 3 * args.steps,

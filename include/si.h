@@ -109,6 +109,10 @@ si_status si_sisi_noalloc(const uint32_t* dA, uint64_t nA, const uint32_t* dB, u
  * last call that used it (SI_OK if none). */
 si_status si_workspace_check(const void* d_workspace, si_stream_t stream);
 
+/* Same, plus where on the device the error was recorded (site: an id of the
+ * bounded wait or check that gave up; detail: site-specific, e.g. a tile). */
+si_status si_workspace_diagnostic(const void* d_workspace, si_stream_t stream, uint32_t* site, uint32_t* detail);
+
 /* Device-side check that x[0..n) is strictly increasing.  Writes 1 (ok) or 0
  * to d_flag (device uint32).  No workspace. */
 si_status si_validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, si_stream_t stream);
@@ -117,9 +121,10 @@ si_status si_validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, 
  * Named cudaEvent pairs around the engine's own kernel launches, recorded on
  * the launching stream while enabled -- the counterpart of the reference's
  * DeviceTimer (include/device_timer.cuh:20-78), which wraps every phase of
- * every executable the same way.  Phase names: "ip_prepare", "ip_split",
- * "ip_tile".  si_timer_read synchronises on the recorded events and returns
- * the summed milliseconds and the number of launches of one phase.
+ * every executable the same way.  Phase names of the single-pair pipeline:
+ * "sisi_prepare", "sisi_split", "sisi_tile".  si_timer_read synchronises on
+ * the recorded events and returns the summed milliseconds and the number of
+ * launches of one phase.
  */
 void si_timer_enable(int on);
 void si_timer_reset(void);

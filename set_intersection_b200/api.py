@@ -66,7 +66,9 @@ class Workspace:
 
     def check(self, stream=None) -> None:
         """Synchronises and raises if the last call recorded a device error."""
-        check(lib.si_workspace_check(_ptr(self.buf), _stream(stream)), "device")
+        site, detail = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        st = lib.si_workspace_diagnostic(_ptr(self.buf), _stream(stream), ctypes.byref(site), ctypes.byref(detail))
+        check(st, f"device (site {site.value}, detail {detail.value})")
 
 
 def sisi_workspace_size(n_a: int, n_b: int, tech="ip") -> int:

@@ -128,6 +128,7 @@ const char* si_last_error_string(void) { return si::g_last_error.c_str(); }
 size_t si_sisi_workspace_size(uint64_t nA, uint64_t nB, si_technique t) {
     switch (t) {
         case SI_TECH_IP:
+        case SI_TECH_BITMAP:
         case SI_TECH_AUTO:
             return si::ip_workspace_size(nA, nB);
         default:
@@ -146,11 +147,12 @@ si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     switch (t) {
         case SI_TECH_IP:
+            return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, d_workspace, workspace_bytes, s, 0);
+        case SI_TECH_BITMAP:
         case SI_TECH_AUTO:
-            return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, d_workspace, workspace_bytes, s);
+            return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, d_workspace, workspace_bytes, s, 1);
         case SI_TECH_OBS:
         case SI_TECH_HI:
-        case SI_TECH_BITMAP:
             return SI_ERR_UNSUPPORTED;
         default:
             return SI_ERR_INVALID_ARGUMENT;
@@ -192,6 +194,17 @@ si_status si_timer_read(const char* phase, double* total_ms, uint64_t* launches)
     *total_ms = sum;
     *launches = n;
     return SI_OK;
+}
+
+si_status si_workspace_diagnostic(const void* d_workspace, si_stream_t stream, uint32_t* site, uint32_t* detail) {
+    if (!d_workspace || !site || !detail) return SI_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t words[3] = {0, 0, 0};
+    SI_CUDA_TRY(cudaMemcpyAsync(words, d_workspace, sizeof(words), cudaMemcpyDeviceToHost, s));
+    SI_CUDA_TRY(cudaStreamSynchronize(s));
+    *site = words[1];
+    *detail = words[2];
+    return static_cast<si_status>(words[0]);
 }
 
 si_status si_validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, si_stream_t stream) {

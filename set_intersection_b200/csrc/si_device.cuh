@@ -11,15 +11,37 @@
 namespace si {
 
 constexpr uint32_t kFullMask = 0xffffffffu;
-// Upper bound on polling iterations of any device-side wait before it gives up
-// and records SI_ERR_TIMEOUT.  With the back-off below this is well over a
-// second of wall time, far beyond any legitimate wait.
-constexpr uint32_t kSpinLimit = 1u << 24;
+// Every device-side wait gives up after this much wall time (read from
+// %globaltimer) and records SI_ERR_TIMEOUT; legitimate waits last micro- to
+// milliseconds.
+constexpr uint64_t kWaitLimitNs = 4000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Deadline helper for a bounded wait: expired() becomes true kWaitLimitNs
+// after construction.
+struct WaitBudget {
+    uint64_t start;
+    uint32_t polls = 0;
+    __device__ __forceinline__ WaitBudget() : start(global_ns()) {}
+    __device__ __forceinline__ bool expired() {
+        // the timer is read every 32 polls
+        return ((++polls & 31u) == 0) && (global_ns() - start > kWaitLimitNs);
+    }
+};
 
 // ---------------------------------------------------------------- errors --
-// The first word of every workspace is the error word: 0 = ok, else si_status.
-__device__ __forceinline__ void record_error(uint32_t* err, si_status code) {
-    atomicCAS(err, 0u, static_cast<uint32_t>(code));
+// The first words of every workspace: [0] error word (0 = ok, else si_status),
+// [1] the site that recorded it, [2] a site-specific detail (e.g. a tile).
+__device__ __forceinline__ void record_error(uint32_t* err, si_status code, uint32_t site = 0, uint32_t info = 0) {
+    if (atomicCAS(err, 0u, static_cast<uint32_t>(code)) == 0u) {
+        err[1] = site;
+        err[2] = info;
+    }
 }
 
 // --------------------------------------------------------------- smem/PTX --
@@ -56,12 +78,40 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait on an mbarrier phase; records SI_ERR_TIMEOUT and returns false
 // if it gives up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err) {
-    for (uint32_t spins = 0; spins < kSpinLimit; ++spins) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err, uint32_t site = 0,
+                                                  uint32_t info = 0) {
+    if (mbar_try_wait(bar, parity)) return true;
+    WaitBudget budget;
+    while (!budget.expired()) {
         if (mbar_try_wait(bar, parity)) return true;
     }
-    record_error(err, SI_ERR_TIMEOUT);
+    record_error(err, SI_ERR_TIMEOUT, site, info);
     return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Orders this thread's earlier generic-proxy shared-memory accesses before its
+// later async-proxy (bulk copy) ones.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Named barrier over `count` threads (id 0 is __syncthreads).
+__device__ __forceinline__ void named_barrier(uint32_t id, uint32_t count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ uint64_t ld_acquire_shared_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.acquire.cta.shared::cta.u64 %0, [%1];" : "=l"(v) : "r"(smem_addr(p)) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_shared_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.release.cta.shared::cta.u64 [%0], %1;" ::"r"(smem_addr(p)), "l"(v) : "memory");
 }
 
 // 1-D bulk copy global -> shared (TMA engine), completion counted on `bar`.
@@ -83,6 +133,19 @@ __device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
 
 __device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Relaxed (unordered) 64-bit accesses at GPU scope: for status words whose
+// flag and value travel together in one word, so no other access needs to be
+// ordered with them.
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 // ------------------------------------------------------------ warp scans --

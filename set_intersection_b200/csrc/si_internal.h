@@ -44,10 +44,11 @@ private:
     cudaStream_t stream_;
 };
 
-// ---- intersect-path SISI (si_sisi_ip.cu) ----
+// ---- single-pair tile pipeline (si_sisi_ip.cu) ----
+// inner: 0 = merge path (technique ip), 1 = bitmap probe (technique bitmap).
 size_t ip_workspace_size(uint64_t nA, uint64_t nB);
 si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
-                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream);
+                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream, int inner = 0);
 
 // ---- sortedness check (si_api.cu) ----
 si_status validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, cudaStream_t stream);

@@ -31,11 +31,6 @@ namespace si {
 namespace {
 
 constexpr uint32_t kS = 4096;                     // pivot (sample) stride
-constexpr int kThreads = 256;                     // threads per tile CTA
-constexpr int kVTMax = (2 * kS) / kThreads;       // merge steps per thread, max
-constexpr int kSlots = kVTMax / 2 + 1;            // match slots per thread
-constexpr int kBufElems = kS + 8;                 // per-set stage buffer (+align, sentinel)
-constexpr size_t kSmemBytes = (2 * kBufElems + kThreads * kSlots) * sizeof(uint32_t);
 constexpr int kPartials = 256;
 
 constexpr uint64_t kFlagAgg = 1ull << 62;
@@ -48,9 +43,9 @@ struct Layout {
     uint64_t nSA = 0, nSB = 0, nTiles = 0;
     size_t off_status = 0, off_split_a = 0, off_split_b = 0, off_sa = 0, off_sb = 0, total = 0;
 };
-// Header: [0] u32 error word, [4] u32 tile ticket, [8] u32 tiles done,
+// Header: [0] u32 error word, [4] u32 error site, [8] u32 error detail,
 // [64, 64 + 8*kPartials) u64 partial counts.
-constexpr size_t kOffTicket = 4, kOffDone = 8, kOffPartials = 64;
+constexpr size_t kOffPartials = 64;
 
 Layout make_layout(uint64_t nA, uint64_t nB) {
     Layout L;
@@ -95,9 +90,10 @@ __device__ __forceinline__ uint64_t upper_bound_g(const uint32_t* __restrict__ x
 __global__ void ip_prepare_kernel(const uint32_t* __restrict__ A, const uint32_t* __restrict__ B,
                                   uint32_t* __restrict__ sa, uint64_t nSA, uint32_t* __restrict__ sb, uint64_t nSB,
                                   uint64_t* __restrict__ zero, uint64_t nzero, uint64_t* __restrict__ split_a,
-                                  uint64_t* __restrict__ split_b, uint64_t nsplit) {
+                                  uint64_t* __restrict__ split_b, uint64_t nsplit, uint64_t* __restrict__ d_count) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t0 == 0) *d_count = 0;
     for (uint64_t k = t0; k < nSA; k += stride) sa[k] = __ldg(A + k * kS);
     for (uint64_t k = t0; k < nSB; k += stride) sb[k] = __ldg(B + k * kS);
     for (uint64_t k = t0; k < nzero; k += stride) zero[k] = 0;
@@ -155,201 +151,497 @@ __global__ void ip_split_kernel(const uint32_t* __restrict__ A, uint64_t nA, con
     }
 }
 
-// K3: one CTA per tile, tiles taken in ticket order (so the look-back only
-// ever waits on CTAs that are already running).
-template <bool kOut>
-__global__ void __launch_bounds__(kThreads) ip_tile_kernel(
+// K3: persistent, warp-specialised tile pipeline.
+//
+//   warps 0..8  consumers: intersect one tile at a time out of the input ring
+//   warp  9     producer:  takes its groups of tiles in order, reads their
+//                          splits, stages each tile's A and B ranges into the
+//                          input ring with the bulk-copy engine
+//   warp 10     output:    per tile, the tile's global offset (a decoupled
+//                          look-back once per group), then copies the tile's
+//                          matches from the output ring to global memory
+//
+// Input ring: a variable-size, in-order circular buffer (a tile takes about
+// |A_t| + |B_t| elements); descriptors pass through kSlots full/empty
+// mbarrier pairs.  Every consumer warp arrives on a tile's empty barrier when
+// done with it; the producer learns which ring space is free from those
+// barriers, in tile order.  Output ring: the same idea for matches.  Groups of
+// kGroup consecutive tiles are dealt round-robin to the CTAs of a cooperative
+// launch, so every CTA is resident and a look-back only ever waits on tiles
+// that running CTAs will finish.
+constexpr int kConsumerWarps = 9;  // 288 threads: odd VT of the largest tile stays <= 31
+constexpr int kConsumers = kConsumerWarps * 32;
+constexpr int kProducerWarp = kConsumerWarps;
+constexpr int kOutputWarp = kConsumerWarps + 1;
+constexpr int kBlock = (kConsumerWarps + 2) * 32;
+constexpr int kCtasPerSm = 2;
+constexpr int kSlots = 8;
+constexpr int kOutQ = 8;
+constexpr int kGroup = 4;                    // consecutive tiles per scheduling unit (one look-back each)
+constexpr uint32_t kInRing = 16384;          // u32: 64 KiB
+constexpr uint32_t kOutRing = 5120;          // u32: 20 KiB
+constexpr uint32_t kBitmapSmemWords = 2048;  // u32 per bitmap buffer (8 KiB); two buffers
+constexpr size_t kSmemBytes = size_t(kInRing + kOutRing + 2 * kBitmapSmemWords) * sizeof(uint32_t);
+constexpr uint32_t kEndTile = 0xffffffffu;
+constexpr uint32_t kConsumerBar = 1;  // named barrier id of the consumer warps
+
+static_assert(2 * (kS + 8) + 16 <= kInRing, "a tile's aligned superset must fit the input ring");
+static_assert(kS <= kOutRing, "one tile's matches must fit the output ring");
+static_assert((((2 * kS + kConsumers - 1) / kConsumers) | 1) <= 31, "per-thread match mask is 32 bits");
+static_assert(kGroup + 1 <= 32, "a group's split entries are held one per lane");
+
+struct InDesc {
+    uint32_t tile;
+    uint32_t offA, offB;  // ring offsets of element 0 of the staged A / B ranges
+    int na, nb;
+    uint32_t fast;        // both successor elements staged: sentinel-terminated merge
+};
+
+struct OutDesc {
+    uint32_t tile;
+    uint32_t off, count;  // output-ring offset and number of matches
+    uint64_t end;         // virtual output-ring offset just past this tile
+};
+
+__device__ __forceinline__ uint64_t look_back(uint64_t* status, uint64_t t, uint32_t* err) {
+    // Warp-wide; returns the exclusive prefix of tile t (t > 0).  Flag and
+    // value share one 64-bit word, so relaxed accesses suffice.
+    const int lane = threadIdx.x & 31;
+    uint64_t prefix = 0;
+    int64_t p = static_cast<int64_t>(t) - 1 - lane;
+    while (true) {
+        uint64_t s = p >= 0 ? ld_relaxed_u64(status + p) : kFlagInc;
+        WaitBudget budget;
+        bool gave_up = false;
+        while (__any_sync(kFullMask, (s >> 62) == 0)) {
+            if ((s >> 62) == 0) {
+                __nanosleep(32);
+                s = ld_relaxed_u64(status + p);
+            }
+            if (__any_sync(kFullMask, budget.expired())) {  // warp-uniform exit
+                gave_up = true;
+                break;
+            }
+        }
+        if (gave_up) {
+            if (lane == 0) record_error(err, SI_ERR_TIMEOUT, 1, static_cast<uint32_t>(t));
+            return prefix;
+        }
+        const uint32_t inc_mask = __ballot_sync(kFullMask, (s >> 62) == 2);
+        const uint64_t v = s & kValMask;
+        if (inc_mask) {
+            const int first = __ffs(inc_mask) - 1;
+            return prefix + warp_sum_u64(lane <= first ? v : 0ull);
+        }
+        prefix += warp_sum_u64(v);
+        p -= 32;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-tile inner algorithms.  Each consumer thread ends with the matches it
+// owns as a bit mask over a contiguous run of one staged set: the matched
+// values are src[start + x] for every set bit x, in ascending order, and the
+// runs of consecutive threads are consecutive.
+enum Inner { kMergePath = 0, kBitmapProbe = 1 };
+
+struct ThreadMatches {
+    const uint32_t* src;
+    int start;
+    uint32_t mask;
+};
+
+// Merge path (the reference's intersect-path, include/helpers.cuh:24-61): the
+// thread takes diagonals [d0, d0 + VT) of the tile's merge of A and B, finds
+// its split with a branch-free binary search (A first on ties) and merges
+// serially; a match is recorded when an A element is consumed while the head
+// of B equals it.
+__device__ __forceinline__ ThreadMatches merge_inner(const uint32_t* sA, int na, const uint32_t* sB, int nb,
+                                                     bool fast, int tid) {
+    const int L = na + nb;
+    // Odd steps per thread: consecutive threads then start VT/2 (a non-integer)
+    // words apart in each set, which spreads their shared loads over the banks.
+    const int VT = ((L + kConsumers - 1) / kConsumers) | 1;
+    const int d0 = min(tid * VT, L), d1 = min(d0 + VT, L);
+    int lo = max(0, d0 - nb), len = min(d0, na) - lo;
+    while (len > 0) {
+        const int half = len >> 1, mid = lo + half;
+        const bool c = sA[mid] <= sB[d0 - 1 - mid];
+        lo = c ? mid + 1 : lo;
+        len = c ? len - half - 1 : half;
+    }
+    const int i0 = lo;
+    uint32_t mask = 0;  // bit x: A element i0 + x is in B
+    if (fast) {
+        // sA[na] / sB[nb] are the successor elements of the ranges, both at or
+        // above the next pivot and so above every value of the tile: they stop
+        // each side without bounds checks.  One shared load per step.
+        const uint32_t* pa = sA + i0;
+        const uint32_t* pb = sB + (d0 - i0);
+        uint32_t a = *pa, b = *pb, bit = 1u;
+        for (int s = d0; s < d1; ++s) {
+            const bool takeA = a <= b;
+            mask |= (a == b) ? bit : 0u;
+            bit = takeA ? bit << 1 : bit;
+            pa += takeA ? 1 : 0;
+            pb += takeA ? 0 : 1;
+            const uint32_t v = *(takeA ? pa : pb);
+            a = takeA ? v : a;
+            b = takeA ? b : v;
+        }
+    } else {
+        int i = i0, j = d0 - i0;
+        for (int s = d0; s < d1; ++s) {
+            const bool aOk = i < na, bOk = j < nb;
+            const uint32_t a = aOk ? sA[i] : 0u, b = bOk ? sB[j] : 0u;
+            const bool takeA = aOk && (!bOk || a <= b);
+            if (takeA && bOk && a == b) mask |= 1u << (i - i0);
+            if (takeA) ++i; else ++j;
+        }
+    }
+    return {sA, i0, mask};
+}
+
+// Bitmap probe (the reference's bitmap_dynamic, src/bitmap_dynamic.cu:240-276,
+// restricted to one tile): the set part with the narrower value span is
+// written as a bitmap of that span into shared memory, the other part probes
+// it.  A tile only holds the values between two pivots, so the span is small
+// for all but very sparse data; a tile whose span exceeds the bitmap falls
+// back to the merge path.  Two bitmap buffers alternate between bitmap tiles:
+// a buffer's words are cleared right before its next use, after the other
+// buffer's tile has passed two barriers, so no thread still probes them.
+constexpr uint32_t kBitmapWords = kBitmapSmemWords;  // a span of up to 65536 values
+__device__ __forceinline__ bool bitmap_fits(const uint32_t* sA, int na, const uint32_t* sB, int nb, bool& buildA,
+                                            uint32_t& span) {
+    if (na == 0 || nb == 0) return false;
+    const uint32_t spanA = sA[na - 1] - sA[0], spanB = sB[nb - 1] - sB[0];
+    buildA = spanA <= spanB;
+    span = buildA ? spanA : spanB;
+    return span < kBitmapWords * 32u;
+}
+
+__device__ __forceinline__ ThreadMatches bitmap_inner(const uint32_t* sA, int na, const uint32_t* sB, int nb,
+                                                      bool buildA, uint32_t span, int tid, uint32_t* bm,
+                                                      uint32_t stale_words) {
+    for (uint32_t w = tid; w < stale_words; w += kConsumers) bm[w] = 0u;
+    named_barrier(kConsumerBar, kConsumers);
+    const uint32_t* X = buildA ? sA : sB;
+    const uint32_t* Y = buildA ? sB : sA;
+    const int nx = buildA ? na : nb, ny = buildA ? nb : na;
+    const uint32_t base = X[0];
+#pragma unroll 4
+    for (int e = tid; e < nx; e += kConsumers) {
+        const uint32_t v = X[e] - base;
+        if (v <= span) atomicOr(bm + (v >> 5), 1u << (v & 31));  // always, for sorted input
+    }
+    named_barrier(kConsumerBar, kConsumers);
+    const int r = ((ny + kConsumers - 1) / kConsumers) | 1;  // <= 15: one part holds <= kS values
+    const int j0 = min(tid * r, ny), j1 = min(j0 + r, ny);
+    uint32_t mask = 0;
+#pragma unroll 4
+    for (int e = j0; e < j1; ++e) {
+        const uint32_t v = Y[e] - base;
+        const uint32_t w = v <= span ? bm[v >> 5] : 0u;
+        mask |= ((w >> (v & 31)) & 1u) << (e - j0);
+    }
+    return {Y, j0, mask};
+}
+
+template <bool kOut, int kInner>
+__global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     const uint32_t* __restrict__ A, uint64_t nA, const uint32_t* __restrict__ B, uint64_t nB,
     const uint64_t* __restrict__ split_a, const uint64_t* __restrict__ split_b, uint64_t nTiles,
     unsigned char* __restrict__ ws, uint64_t* __restrict__ status, uint32_t* __restrict__ out, uint64_t out_cap,
     uint64_t* __restrict__ d_count) {
     extern __shared__ __align__(16) uint32_t smem[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_warp[kThreads / 32];
-    __shared__ uint64_t s_prefix;
-    __shared__ uint32_t s_last;
+    uint32_t* in_ring = smem;
+    uint32_t* out_ring = smem + kInRing;
+    uint32_t* bitmaps = smem + kInRing + kOutRing;  // 2 x kBitmapSmemWords
+    __shared__ __align__(8) uint64_t full[kSlots], empty[kSlots], ofull[kOutQ], oempty[kOutQ];
+    __shared__ InDesc in_desc[kSlots];
+    __shared__ uint64_t s_in_end[kSlots];  // producer-private: ring end of the tile in each slot
+    __shared__ OutDesc out_desc[kOutQ];
+    __shared__ __align__(8) uint64_t s_released_out;
+    __shared__ uint32_t s_warp[2][kConsumerWarps];  // by tile parity: a warp may run one tile ahead
+    __shared__ uint32_t s_ooff;
 
     uint32_t* err = reinterpret_cast<uint32_t*>(ws);
-    uint32_t* ticket = reinterpret_cast<uint32_t*>(ws + kOffTicket);
-    uint32_t* done = reinterpret_cast<uint32_t*>(ws + kOffDone);
-    uint64_t* partials = reinterpret_cast<uint64_t*>(ws + kOffPartials);
-
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    uint32_t* bufA = smem;
-    uint32_t* bufB = smem + kBufElems;
-    uint32_t* slots = smem + 2 * kBufElems;
-
+    if constexpr (kInner == kBitmapProbe) {
+        for (uint32_t w = tid; w < 2 * kBitmapSmemWords; w += kBlock) bitmaps[w] = 0u;
+    }
     if (tid == 0) {
-        mbar_init(&bar, 1);
+        for (int i = 0; i < kSlots; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], kConsumerWarps);
+        }
+        for (int i = 0; i < kOutQ; ++i) {
+            mbar_init(&ofull[i], 1);
+            mbar_init(&oempty[i], 1);
+        }
+        s_released_out = 0;
         fence_mbar_init();
-        s_tile = atomicAdd(ticket, 1u);
     }
     __syncthreads();
-    const uint64_t t = s_tile;
 
-    uint64_t a0 = split_a[t], a1 = split_a[t + 1], b0 = split_b[t], b1 = split_b[t + 1];
-    const bool ok = a0 <= a1 && a1 <= nA && a1 - a0 <= kS && b0 <= b1 && b1 <= nB && b1 - b0 <= kS;
-    if (!ok) {
-        if (tid == 0) record_error(err, SI_ERR_INVALID_INPUT);
-        a0 = a1 = b0 = b1 = 0;
-    }
-    const int na = static_cast<int>(a1 - a0), nb = static_cast<int>(b1 - b0);
-    const uint32_t* gA = A + a0;
-    const uint32_t* gB = B + b0;
-    const StagePlan pa = plan_stage(gA, na, bufA);
-    const StagePlan pb = plan_stage(gB, nb, bufB);
-    if (tid == 0) {
-        mbar_arrive_expect_tx(&bar, static_cast<uint32_t>(pa.body + pb.body) * 4u);
-        issue_stage(pa, gA, &bar);
-        issue_stage(pb, gB, &bar);
-    }
-    if (tid < 6) edge_stage(pa, gA, tid);
-    else if (tid >= 32 && tid < 38) edge_stage(pb, gB, tid - 32);
-    else if (tid == 64) pa.dst[na] = 0xffffffffu;  // sentinels
-    else if (tid == 65) pb.dst[nb] = 0xffffffffu;
-    mbar_wait_bounded(&bar, 0, err);
-    __syncthreads();
-
-    // ---- thread-level merge path ----
-    const uint32_t* sA = pa.dst;
-    const uint32_t* sB = pb.dst;
-    const int L = na + nb;
-    const int VT = (L + kThreads - 1) / kThreads;
-    const int d0 = min(tid * VT, L), d1 = min(d0 + VT, L);
-    int lo = max(0, d0 - nb), hi = min(d0, na);
-    while (lo < hi) {  // A first on ties: A[mid] precedes B[d0-1-mid] iff A[mid] <= B[d0-1-mid]
-        const int mid = (lo + hi) >> 1;
-        if (sA[mid] <= sB[d0 - 1 - mid]) lo = mid + 1; else hi = mid;
-    }
-    int i = lo, j = d0 - lo;
-    uint32_t* my = slots + tid * kSlots;
-    int cnt = 0;
-    if (t + 1 < nTiles) {
-        // Every value of a non-final tile is below the next pivot, hence below
-        // 0xffffffff: the sentinels terminate each side without bounds checks.
-        uint32_t a = sA[i], b = sB[j];
-        for (int s = d0; s < d1; ++s) {
-            if (a == b) {
-                my[cnt < kSlots ? cnt : kSlots - 1] = a;
-                ++cnt;
+    if (warp == kProducerWarp) {
+        // ------------------------------------------------------ producer --
+        // This CTA takes groups blockIdx.x, blockIdx.x + gridDim.x, ...; the
+        // split entries of the next group load while the current one stages.
+        // Lane x computes the staging parameters of the group's tile x.
+        uint64_t head = 0, released = 0;  // virtual ring offsets (lane 0)
+        uint32_t k = 0, k_rel = 0;        // tiles staged / tiles known released
+        bool done = false;
+        auto load_splits = [&](uint64_t grp, uint64_t& sa_, uint64_t& sb_) {
+            const uint64_t idx = grp * kGroup + lane;
+            sa_ = (lane <= kGroup && idx <= nTiles) ? split_a[idx] : 0;
+            sb_ = (lane <= kGroup && idx <= nTiles) ? split_b[idx] : 0;
+        };
+        // lane 0: wait for the oldest staged tile to be released by every consumer warp
+        auto wait_release = [&]() -> bool {
+            const uint32_t sl = k_rel % kSlots;
+            if (!mbar_wait_bounded(&empty[sl], (k_rel / kSlots) & 1, err, 2, k_rel)) return false;
+            released = s_in_end[sl];
+            ++k_rel;
+            return true;
+        };
+        uint64_t g = blockIdx.x;
+        uint64_t sp_a, sp_b;
+        load_splits(g, sp_a, sp_b);
+        while (!done) {
+            const uint64_t t_first = g * kGroup;
+            const uint64_t gn = g + gridDim.x;
+            uint64_t nsp_a, nsp_b;
+            load_splits(gn, nsp_a, nsp_b);  // in flight while this group is staged
+            // ---- lane x: parameters of tile t_first + x ----
+            uint64_t a0 = __shfl_sync(kFullMask, sp_a, lane < kGroup ? lane : 0);
+            uint64_t a1 = __shfl_sync(kFullMask, sp_a, lane < kGroup ? lane + 1 : 1);
+            uint64_t b0 = __shfl_sync(kFullMask, sp_b, lane < kGroup ? lane : 0);
+            uint64_t b1 = __shfl_sync(kFullMask, sp_b, lane < kGroup ? lane + 1 : 1);
+            const bool ok = a0 <= a1 && a1 <= nA && a1 - a0 <= kS && b0 <= b1 && b1 <= nB && b1 - b0 <= kS;
+            const uint64_t t_mine = t_first + lane;
+            if (!ok && lane < kGroup && t_mine < nTiles) record_error(err, SI_ERR_INVALID_INPUT);
+            if (!ok) a0 = a1 = b0 = b1 = 0;
+            // 16-byte aligned superset of [x0, x1] (x1, the successor element
+            // when it exists, doubles as the merge sentinel).  Every 16-byte
+            // block copied holds at least one element of the range.
+            const uint64_t aEnd = a1 < nA ? a1 + 1 : a1, bEnd = b1 < nB ? b1 + 1 : b1;
+            const uintptr_t a_lo = reinterpret_cast<uintptr_t>(A + a0) & ~uintptr_t(15);
+            const uintptr_t b_lo = reinterpret_cast<uintptr_t>(B + b0) & ~uintptr_t(15);
+            const uint32_t bytesA =
+                aEnd > a0 ? static_cast<uint32_t>(((reinterpret_cast<uintptr_t>(A + aEnd) + 15) & ~uintptr_t(15)) - a_lo)
+                          : 0u;
+            const uint32_t bytesB =
+                bEnd > b0 ? static_cast<uint32_t>(((reinterpret_cast<uintptr_t>(B + bEnd) + 15) & ~uintptr_t(15)) - b_lo)
+                          : 0u;
+            const uint32_t needA = bytesA / 4 + 4, needB = bytesB / 4 + 4;  // (+4: room for misalignment)
+            const uint32_t misA = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(A + a0) & 15u) >> 2);
+            const uint32_t misB = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(B + b0) & 15u) >> 2);
+            const uint32_t fast = (t_mine + 1 < nTiles) && a1 < nA && b1 < nB;
+            for (int x = 0; x < kGroup; ++x) {
+                const uint64_t t = t_first + x;
+                const uint32_t slot = k % kSlots;
+                const uint64_t xa_lo = __shfl_sync(kFullMask, static_cast<uint64_t>(a_lo), x);
+                const uint64_t xb_lo = __shfl_sync(kFullMask, static_cast<uint64_t>(b_lo), x);
+                const uint32_t xbytesA = __shfl_sync(kFullMask, bytesA, x), xbytesB = __shfl_sync(kFullMask, bytesB, x);
+                const uint32_t xneedA = __shfl_sync(kFullMask, needA, x), xneedB = __shfl_sync(kFullMask, needB, x);
+                const uint32_t xmisA = __shfl_sync(kFullMask, misA, x), xmisB = __shfl_sync(kFullMask, misB, x);
+                const uint32_t xna = __shfl_sync(kFullMask, static_cast<uint32_t>(a1 - a0), x);
+                const uint32_t xnb = __shfl_sync(kFullMask, static_cast<uint32_t>(b1 - b0), x);
+                const uint32_t xfast = __shfl_sync(kFullMask, fast, x);
+                if (lane == 0) {
+                    // the slot's previous tile (k - kSlots) must be released by
+                    // every consumer warp before the slot is written, also for
+                    // the end marker
+                    bool alive = true;
+                    while (alive && k_rel + kSlots <= k) alive = wait_release();
+                    const bool slot_free = alive;
+                    alive = alive && t < nTiles;
+                    const uint32_t need = xneedA + xneedB;
+                    if (alive) {
+                        // A tile never wraps: if it does not fit before the ring's end it
+                        // starts the next lap.  It may be placed once it overlaps no live
+                        // tile: either every staged tile is released, or the live span
+                        // [released, head) ends at least kInRing before the tile's end.
+                        const uint64_t phys = head % kInRing;
+                        if (phys + need > kInRing) head += kInRing - phys;
+                        while (alive && k_rel < k && head + need - released > kInRing) alive = wait_release();
+                    }
+                    if (!alive) {
+                        if (t < nTiles) record_error(err, SI_ERR_TIMEOUT, 3, static_cast<uint32_t>(t));
+                        if (slot_free) {  // else the consumers' own bounded waits end them
+                            in_desc[slot].tile = kEndTile;
+                            mbar_arrive(&full[slot]);
+                        }
+                    } else {
+                        const uint32_t base = static_cast<uint32_t>(head % kInRing);
+                        head += need;
+                        s_in_end[slot] = head;
+                        InDesc& d = in_desc[slot];
+                        d.tile = static_cast<uint32_t>(t);
+                        d.offA = base + xmisA;
+                        d.offB = base + xneedA + xmisB;
+                        d.na = static_cast<int>(xna);
+                        d.nb = static_cast<int>(xnb);
+                        d.fast = xfast;
+                        mbar_arrive_expect_tx(&full[slot], xbytesA + xbytesB);
+                        if (xbytesA) bulk_g2s(in_ring + base, reinterpret_cast<const void*>(xa_lo), xbytesA, &full[slot]);
+                        if (xbytesB)
+                            bulk_g2s(in_ring + base + xneedA, reinterpret_cast<const void*>(xb_lo), xbytesB, &full[slot]);
+                    }
+                    done = !alive;
+                }
+                done = __shfl_sync(kFullMask, done ? 1u : 0u, 0) != 0;
+                if (done) break;
+                ++k;
             }
-            if (a <= b) a = sA[++i]; else b = sB[++j];
+            g = gn;
+            sp_a = nsp_a;
+            sp_b = nsp_b;
         }
-    } else {
-        // Final tile: may hold the value 0xffffffff, so check bounds explicitly.
-        for (int s = d0; s < d1; ++s) {
-            const bool aOk = i < na, bOk = j < nb;
-            const uint32_t a = aOk ? sA[i] : 0u, b = bOk ? sB[j] : 0u;
-            const bool takeA = aOk && (!bOk || a <= b);
-            if (takeA && bOk && a == b) {
-                my[cnt < kSlots ? cnt : kSlots - 1] = a;
-                ++cnt;
-            }
-            if (takeA) ++i; else ++j;
-        }
-    }
-    if (cnt > kSlots) {  // only possible for input that is not strictly increasing
-        record_error(err, SI_ERR_INVALID_INPUT);
-        cnt = kSlots;
+        return;
     }
 
-    // ---- block scan of per-thread match counts ----
-    const uint32_t incl = warp_inclusive_scan(static_cast<uint32_t>(cnt));
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t v = lane < kThreads / 32 ? s_warp[lane] : 0u;
-        v = warp_inclusive_scan(v);
-        if (lane < kThreads / 32) s_warp[lane] = v;
-    }
-    __syncthreads();
-    const uint32_t excl = incl - static_cast<uint32_t>(cnt) + (warp ? s_warp[warp - 1] : 0u);
-    const uint32_t tile_count = s_warp[kThreads / 32 - 1];
-
-    if constexpr (!kOut) {
-        if (tid == 0) {
-            atomicAdd(reinterpret_cast<unsigned long long*>(partials + (t & (kPartials - 1))),
-                      static_cast<unsigned long long>(tile_count));
-            __threadfence();
-            s_last = (atomicAdd(done, 1u) == nTiles - 1) ? 1u : 0u;
-        }
-        __syncthreads();
-        if (s_last) {
-            __threadfence();
-            uint64_t v = 0;
-            for (int x = tid; x < kPartials; x += kThreads) v += ld_acquire_u64(partials + x);
-            v = warp_sum_u64(v);
-            __shared__ uint64_t s_sum[kThreads / 32];
-            if (lane == 0) s_sum[warp] = v;
-            __syncthreads();
-            if (tid == 0) {
-                uint64_t total = 0;
-                for (int w = 0; w < kThreads / 32; ++w) total += s_sum[w];
-                *d_count = total;
+    if (warp == kOutputWarp) {
+        // -------------------------------------------------------- output --
+        // One look-back per group (its first tile); later tiles of the group
+        // follow from the running prefix.
+        if constexpr (kOut) {
+            uint64_t prefix = 0;
+            for (uint32_t k = 0;; ++k) {
+                const uint32_t j = k % kOutQ, round = k / kOutQ;
+                if (!mbar_wait_bounded(&ofull[j], round & 1, err, 4, k)) break;
+                const OutDesc d = out_desc[j];
+                if (d.tile == kEndTile) break;
+                if (d.tile % kGroup == 0) prefix = d.tile > 0 ? look_back(status, d.tile, err) : 0;
+                if (d.tile > 0 && lane == 0) st_relaxed_u64(status + d.tile, kFlagInc | ((prefix + d.count) & kValMask));
+                bool overflow = false;
+                for (uint32_t x = lane; x < d.count; x += 32) {
+                    const uint64_t pos = prefix + x;
+                    if (pos < out_cap) out[pos] = out_ring[d.off + x];
+                    else overflow = true;
+                }
+                if (overflow) record_error(err, SI_ERR_OUTPUT_OVERFLOW);
+                prefix += d.count;
+                if (lane == 0 && d.tile + 1 == nTiles) *d_count = prefix;
+                __syncwarp();
+                if (lane == 0) {
+                    st_release_shared_u64(&s_released_out, d.end);
+                    mbar_arrive(&oempty[j]);
+                }
             }
         }
         return;
-    } else {
-        // Compact this tile's matches into the (now free) A stage buffer.
-        uint32_t* comp = bufA;
-        for (int c = 0; c < cnt; ++c) comp[excl + c] = my[c];
+    }
 
-        if (warp == 0) {
-            uint64_t prefix = 0;
-            if (t == 0) {
-                if (lane == 0) st_release_u64(status, kFlagInc | tile_count);
-            } else {
-                if (lane == 0) st_release_u64(status + t, kFlagAgg | tile_count);
-                int64_t p = static_cast<int64_t>(t) - 1 - lane;
-                bool gave_up = false;
-                while (true) {
-                    uint64_t s = p >= 0 ? ld_acquire_u64(status + p) : kFlagInc;
-                    uint32_t spins = 0;
-                    while (__any_sync(kFullMask, (s >> 62) == 0)) {
-                        if ((s >> 62) == 0) {
-                            __nanosleep(64);
-                            s = ld_acquire_u64(status + p);
-                        }
-                        if (++spins > kSpinLimit) { gave_up = true; break; }
-                    }
-                    if (__any_sync(kFullMask, gave_up)) {
-                        if (lane == 0) record_error(err, SI_ERR_TIMEOUT);
-                        break;
-                    }
-                    const uint32_t inc_mask = __ballot_sync(kFullMask, (s >> 62) == 2);
-                    uint64_t v = s & kValMask;
-                    if (inc_mask) {
-                        const int first = __ffs(inc_mask) - 1;
-                        prefix += warp_sum_u64(lane <= first ? v : 0ull);
-                        break;
-                    }
-                    prefix += warp_sum_u64(v);
-                    p -= 32;
-                }
-                if (lane == 0) st_release_u64(status + t, kFlagInc | ((prefix + tile_count) & kValMask));
+    // ---------------------------------------------------------- consumers --
+    uint64_t my_count = 0;     // count-only: this thread's matches over all its tiles
+    uint64_t ohead = 0;        // thread 0: virtual output-ring head
+    uint32_t stale0 = 0u, stale1 = 0u;  // bitmap words left set in each buffer
+    uint32_t nbm = 0;          // bitmap tiles so far (buffer parity)
+    uint32_t k = 0;            // tiles consumed so far = index of the next output-queue entry
+    for (;; ++k) {
+        const uint32_t slot = k % kSlots;
+        if (!mbar_wait_bounded(&full[slot], (k / kSlots) & 1, err, 5, k)) break;
+        const InDesc d = in_desc[slot];
+        if (d.tile == kEndTile) break;
+        const uint32_t* sA = in_ring + d.offA;
+        const uint32_t* sB = in_ring + d.offB;
+        ThreadMatches tm;
+        bool buildA = true;
+        uint32_t span = 0;
+        if (kInner == kBitmapProbe && bitmap_fits(sA, d.na, sB, d.nb, buildA, span)) {
+            const uint32_t buf = nbm & 1u;
+            tm = bitmap_inner(sA, d.na, sB, d.nb, buildA, span, tid, bitmaps + buf * kBitmapSmemWords,
+                              buf ? stale1 : stale0);
+            if (buf) stale1 = (span >> 5) + 1; else stale0 = (span >> 5) + 1;
+            ++nbm;
+        } else {
+            tm = merge_inner(sA, d.na, sB, d.nb, d.fast != 0, tid);
+        }
+        const uint32_t cnt = static_cast<uint32_t>(__popc(tm.mask));
+
+        if constexpr (!kOut) {
+            my_count += cnt;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[slot]);  // this warp is done with the tile
+            continue;
+        } else {
+            // block scan over the consumer warps
+            const uint32_t incl = warp_inclusive_scan(cnt);
+            if (lane == 31) s_warp[k & 1][warp] = incl;
+            named_barrier(kConsumerBar, kConsumers);
+            uint32_t wsum = 0, tile_count = 0;
+#pragma unroll
+            for (int w = 0; w < kConsumerWarps; ++w) {
+                const uint32_t v = s_warp[k & 1][w];
+                wsum += w < warp ? v : 0u;
+                tile_count += v;
             }
-            if (lane == 0) s_prefix = prefix;
+            const uint32_t excl = incl - cnt + wsum;
+            // the tile's aggregate goes out at once, for later tiles' look-backs
+            if (tid == 32) st_relaxed_u64(status + d.tile, (d.tile == 0 ? kFlagInc : kFlagAgg) | tile_count);
+            if (tid == 0) {
+                // same placement rule as the input ring (a skipped tail is free
+                // once every earlier tile has been written out)
+                const uint64_t live_end = ohead;
+                const uint64_t ophys = ohead % kOutRing;
+                if (ophys + tile_count > kOutRing) ohead += kOutRing - ophys;
+                bool space = false;
+                for (WaitBudget budget; !budget.expired();) {
+                    const uint64_t rel = ld_acquire_shared_u64(&s_released_out);
+                    if (rel >= live_end || ohead + tile_count - rel <= kOutRing) {
+                        space = true;
+                        break;
+                    }
+                    __nanosleep(20);
+                }
+                if (!space) record_error(err, SI_ERR_TIMEOUT, 6, d.tile);
+                s_ooff = space ? static_cast<uint32_t>(ohead % kOutRing) : kEndTile;
+                ohead += tile_count;
+            }
+            named_barrier(kConsumerBar, kConsumers);
+            const uint32_t ooff = s_ooff;
+            if (ooff == kEndTile) break;  // gave up waiting for output space (error recorded)
+            uint32_t m = tm.mask, c = excl;
+            while (m) {
+                const int x = __ffs(m) - 1;
+                m &= m - 1;
+                out_ring[ooff + c++] = tm.src[tm.start + x];
+            }
+            named_barrier(kConsumerBar, kConsumers);  // all matches written, tile no longer read
+            if (lane == 0) mbar_arrive(&empty[slot]);
+            if (tid == 0) {
+                const uint32_t q = k % kOutQ;
+                mbar_wait_bounded(&oempty[q], ((k / kOutQ) & 1) ^ 1, err, 7, k);
+                OutDesc& od = out_desc[q];
+                od.tile = d.tile;
+                od.off = ooff;
+                od.count = tile_count;
+                od.end = ohead;
+                mbar_arrive(&ofull[q]);
+            }
         }
-        __syncthreads();
-        const uint64_t base = s_prefix;
-        bool overflow = false;
-        for (uint32_t x = tid; x < tile_count; x += kThreads) {
-            const uint64_t pos = base + x;
-            if (pos < out_cap) out[pos] = comp[x];
-            else overflow = true;
+    }
+    if constexpr (kOut) {
+        if (tid == 0) {  // end marker for the output warp
+            const uint32_t q = k % kOutQ;
+            if (mbar_wait_bounded(&oempty[q], ((k / kOutQ) & 1) ^ 1, err, 8, k)) {
+                out_desc[q].tile = kEndTile;
+                mbar_arrive(&ofull[q]);
+            }
         }
-        if (overflow) record_error(err, SI_ERR_OUTPUT_OVERFLOW);
-        if (tid == 0 && t + 1 == nTiles) *d_count = base + tile_count;
+    } else {
+        const uint64_t wsum = warp_sum_u64(my_count);
+        if (lane == 0 && wsum) atomicAdd(reinterpret_cast<unsigned long long*>(d_count), wsum);
     }
 }
-
 }  // namespace
 
 size_t ip_workspace_size(uint64_t nA, uint64_t nB) { return make_layout(nA, nB).total; }
 
 si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
-                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream) {
+                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream, int inner) {
     const Layout L = make_layout(nA, nB);
     if (ws_bytes < L.total) return SI_ERR_WORKSPACE_TOO_SMALL;
     if (L.nTiles > 0x7fffffffull) return SI_ERR_INVALID_ARGUMENT;
@@ -365,33 +657,46 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
     const unsigned grid1 =
         static_cast<unsigned>(std::min<uint64_t>((work1 + 255) / 256, static_cast<uint64_t>(sm_count()) * 8));
     {
-    PhaseTimer timer("ip_prepare", stream);
+    PhaseTimer timer("sisi_prepare", stream);
     ip_prepare_kernel<<<grid1, 256, 0, stream>>>(dA, dB, sa, L.nSA, sb, L.nSB, reinterpret_cast<uint64_t*>(w), nzero,
-                                                 split_a, split_b, L.nTiles + 1);
+                                                 split_a, split_b, L.nTiles + 1, d_count);
     SI_LAUNCH_CHECK("ip_prepare_kernel");
     }
 
     const uint64_t nP = L.nSA + L.nSB;
     const unsigned grid2 = static_cast<unsigned>(std::max<uint64_t>(1, (nP + 255) / 256));
     {
-    PhaseTimer timer("ip_split", stream);
+    PhaseTimer timer("sisi_split", stream);
     ip_split_kernel<<<grid2, 256, 0, stream>>>(dA, nA, dB, nB, sa, L.nSA, sb, L.nSB, split_a, split_b);
     SI_LAUNCH_CHECK("ip_split_kernel");
     }
 
-    SI_CUDA_TRY(cudaFuncSetAttribute(ip_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kSmemBytes)));
-    SI_CUDA_TRY(cudaFuncSetAttribute(ip_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kSmemBytes)));
-    PhaseTimer timer("ip_tile", stream);
-    if (d_out) {
-        ip_tile_kernel<true><<<static_cast<unsigned>(L.nTiles), kThreads, kSmemBytes, stream>>>(
-            dA, nA, dB, nB, split_a, split_b, L.nTiles, w, status, d_out, out_cap, d_count);
+    const uint64_t nGroups = (L.nTiles + kGroup - 1) / kGroup;
+    auto launch = [&](auto kernel, uint32_t* out) -> si_status {
+        SI_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kSmemBytes)));
+        int per_sm = 0;
+        SI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, kSmemBytes));
+        if (per_sm < 1) return SI_ERR_UNSUPPORTED;
+        const unsigned grid =
+            static_cast<unsigned>(std::min<uint64_t>(nGroups, static_cast<uint64_t>(sm_count()) * per_sm));
+        uint64_t cap = out ? out_cap : 0;
+        uint64_t nTiles = L.nTiles;
+        void* args[] = {(void*)&dA, (void*)&nA, (void*)&dB, (void*)&nB, (void*)&split_a, (void*)&split_b,
+                        (void*)&nTiles, (void*)&w, (void*)&status, (void*)&out, (void*)&cap, (void*)&d_count};
+        PhaseTimer timer("sisi_tile", stream);
+        SI_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(grid), dim3(kBlock), args,
+                                                kSmemBytes, stream));
+        return SI_OK;
+    };
+    si_status st;
+    if (inner == kBitmapProbe) {
+        st = d_out ? launch(ip_tile_kernel<true, kBitmapProbe>, d_out) : launch(ip_tile_kernel<false, kBitmapProbe>, nullptr);
     } else {
-        ip_tile_kernel<false><<<static_cast<unsigned>(L.nTiles), kThreads, kSmemBytes, stream>>>(
-            dA, nA, dB, nB, split_a, split_b, L.nTiles, w, status, nullptr, 0, d_count);
+        st = d_out ? launch(ip_tile_kernel<true, kMergePath>, d_out) : launch(ip_tile_kernel<false, kMergePath>, nullptr);
     }
-    SI_LAUNCH_CHECK("ip_tile_kernel");
+    if (st != SI_OK) return st;
+    SI_LAUNCH_CHECK("sisi_tile_kernel");
     return SI_OK;
 }
 

@@ -9,7 +9,7 @@ from set_intersection_b200 import dataset as fmt
 
 pytestmark = pytest.mark.gpu
 
-TECHS = ["ip"]
+TECHS = ["ip", "bitmap"]
 
 
 def dev(x):
@@ -153,6 +153,20 @@ def test_full_size_2_28(cuda, tech):
     c, got = run(a, b, tech)
     assert c == want.size
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+@pytest.mark.parametrize("gap", [1, 2, 8, 30, 31, 33, 64, 1 << 12, 1 << 20])
+def test_value_span_per_tile(cuda, tech, gap):
+    """Tiles whose value span is below, at and above the bitmap capacity
+    (65536 values): the bitmap technique must fall back to the merge path
+    exactly where its bitmap cannot hold the span."""
+    rng = np.random.default_rng(gap)
+    n = 60000
+    hi = min(n * gap * 2, 1 << 32)
+    a = _u(rng, n, hi)
+    b = np.unique(np.concatenate([_u(rng, n, hi), a[::3]])).astype(np.uint32)
+    check(a, b, tech)
 
 
 def test_validate_sorted(cuda):
