@@ -37,11 +37,13 @@ struct WaitBudget {
 // ---------------------------------------------------------------- errors --
 // The first words of every workspace: [0] error word (0 = ok, else si_status),
 // [1] the site that recorded it, [2] a site-specific detail (e.g. a tile).
+// [3] is the set of all sites that recorded an error (bit per site id < 32).
 __device__ __forceinline__ void record_error(uint32_t* err, si_status code, uint32_t site = 0, uint32_t info = 0) {
     if (atomicCAS(err, 0u, static_cast<uint32_t>(code)) == 0u) {
         err[1] = site;
         err[2] = info;
     }
+    atomicOr(err + 3, 1u << (site & 31u));
 }
 
 // --------------------------------------------------------------- smem/PTX --

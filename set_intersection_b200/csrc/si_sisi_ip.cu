@@ -44,8 +44,9 @@ struct Layout {
     size_t off_status = 0, off_split_a = 0, off_split_b = 0, off_sa = 0, off_sb = 0, total = 0;
 };
 // Header: [0] u32 error word, [4] u32 error site, [8] u32 error detail,
+// [12] u32 sites that gave up, [16] u32 group ticket,
 // [64, 64 + 8*kPartials) u64 partial counts.
-constexpr size_t kOffPartials = 64;
+constexpr size_t kOffTicket = 16, kOffPartials = 64;
 
 Layout make_layout(uint64_t nA, uint64_t nB) {
     Layout L;
@@ -157,18 +158,23 @@ __global__ void ip_split_kernel(const uint32_t* __restrict__ A, uint64_t nA, con
 //   warp  9     producer:  takes its groups of tiles in order, reads their
 //                          splits, stages each tile's A and B ranges into the
 //                          input ring with the bulk-copy engine
-//   warp 10     output:    per tile, the tile's global offset (a decoupled
-//                          look-back once per group), then copies the tile's
-//                          matches from the output ring to global memory
+//   warp 10     output:    per tile, the tile's global output offset (a
+//                          decoupled look-back once per group, then a running
+//                          sum), then copies the tile's matches from the
+//                          output ring to global memory
 //
 // Input ring: a variable-size, in-order circular buffer (a tile takes about
 // |A_t| + |B_t| elements); descriptors pass through kSlots full/empty
 // mbarrier pairs.  Every consumer warp arrives on a tile's empty barrier when
 // done with it; the producer learns which ring space is free from those
-// barriers, in tile order.  Output ring: the same idea for matches.  Groups of
-// kGroup consecutive tiles are dealt round-robin to the CTAs of a cooperative
-// launch, so every CTA is resident and a look-back only ever waits on tiles
-// that running CTAs will finish.
+// barriers, in tile order.  With element output, consumers write a tile's
+// matches into an output ring (power-of-two, indexed modulo its size, so every
+// consumer thread tracks its head without a broadcast) and release the input
+// tile at once; the output warp places them once the tile's offset is known.
+// Offsets therefore never hold up merging.  Groups of
+// kGroup consecutive tiles are handed out by a ticket counter, so a
+// look-back only ever waits on tiles owned by CTAs that are already running
+// (the launch is also cooperative: every CTA is resident).
 constexpr int kConsumerWarps = 9;  // 288 threads: odd VT of the largest tile stays <= 31
 constexpr int kConsumers = kConsumerWarps * 32;
 constexpr int kProducerWarp = kConsumerWarps;
@@ -176,17 +182,18 @@ constexpr int kOutputWarp = kConsumerWarps + 1;
 constexpr int kBlock = (kConsumerWarps + 2) * 32;
 constexpr int kCtasPerSm = 2;
 constexpr int kSlots = 8;
-constexpr int kOutQ = 8;
+constexpr int kOutQ = 16;                    // output descriptors in flight
 constexpr int kGroup = 4;                    // consecutive tiles per scheduling unit (one look-back each)
-constexpr uint32_t kInRing = 16384;          // u32: 64 KiB
-constexpr uint32_t kOutRing = 5120;          // u32: 20 KiB
+constexpr uint32_t kInRing = 14336;          // u32: 56 KiB
+constexpr uint32_t kOutRing = 4096;          // u32: 16 KiB, a power of two
 constexpr uint32_t kBitmapSmemWords = 2048;  // u32 per bitmap buffer (8 KiB); two buffers
 constexpr size_t kSmemBytes = size_t(kInRing + kOutRing + 2 * kBitmapSmemWords) * sizeof(uint32_t);
+static_assert((kOutRing & (kOutRing - 1)) == 0, "output ring is indexed modulo its size");
+static_assert(kS <= kOutRing, "one tile's matches must fit the output ring");
 constexpr uint32_t kEndTile = 0xffffffffu;
 constexpr uint32_t kConsumerBar = 1;  // named barrier id of the consumer warps
 
 static_assert(2 * (kS + 8) + 16 <= kInRing, "a tile's aligned superset must fit the input ring");
-static_assert(kS <= kOutRing, "one tile's matches must fit the output ring");
 static_assert((((2 * kS + kConsumers - 1) / kConsumers) | 1) <= 31, "per-thread match mask is 32 bits");
 static_assert(kGroup + 1 <= 32, "a group's split entries are held one per lane");
 
@@ -197,44 +204,58 @@ struct InDesc {
     uint32_t fast;        // both successor elements staged: sentinel-terminated merge
 };
 
-struct OutDesc {
-    uint32_t tile;
-    uint32_t off, count;  // output-ring offset and number of matches
-    uint64_t end;         // virtual output-ring offset just past this tile
-};
-
+constexpr int kLookBackPerLane = 4;  // status words per lane per round trip
 __device__ __forceinline__ uint64_t look_back(uint64_t* status, uint64_t t, uint32_t* err) {
     // Warp-wide; returns the exclusive prefix of tile t (t > 0).  Flag and
-    // value share one 64-bit word, so relaxed accesses suffice.
+    // value share one 64-bit word, so relaxed accesses suffice.  Each round
+    // trip reads the 128 nearest unvisited predecessors, lane l holding
+    // tiles base - 4l - 1 ... base - 4l - 4.
     const int lane = threadIdx.x & 31;
     uint64_t prefix = 0;
-    int64_t p = static_cast<int64_t>(t) - 1 - lane;
+    int64_t base = static_cast<int64_t>(t);
     while (true) {
-        uint64_t s = p >= 0 ? ld_relaxed_u64(status + p) : kFlagInc;
+        uint64_t s[kLookBackPerLane];
         WaitBudget budget;
         bool gave_up = false;
-        while (__any_sync(kFullMask, (s >> 62) == 0)) {
-            if ((s >> 62) == 0) {
-                __nanosleep(32);
-                s = ld_relaxed_u64(status + p);
+        while (true) {
+            bool pending = false;
+#pragma unroll
+            for (int q = 0; q < kLookBackPerLane; ++q) {
+                const int64_t p = base - 1 - lane * kLookBackPerLane - q;
+                s[q] = p >= 0 ? ld_relaxed_u64(status + p) : kFlagInc;
+                pending |= (s[q] >> 62) == 0;
             }
+            if (!__any_sync(kFullMask, pending)) break;
             if (__any_sync(kFullMask, budget.expired())) {  // warp-uniform exit
                 gave_up = true;
                 break;
             }
+            __nanosleep(32);
         }
         if (gave_up) {
             if (lane == 0) record_error(err, SI_ERR_TIMEOUT, 1, static_cast<uint32_t>(t));
             return prefix;
         }
-        const uint32_t inc_mask = __ballot_sync(kFullMask, (s >> 62) == 2);
-        const uint64_t v = s & kValMask;
+        // nearest inclusive status in this window: lane-major, then q
+        int first_q = kLookBackPerLane;
+#pragma unroll
+        for (int q = kLookBackPerLane - 1; q >= 0; --q)
+            if ((s[q] >> 62) == 2) first_q = q;
+        const uint32_t inc_mask = __ballot_sync(kFullMask, first_q < kLookBackPerLane);
+        uint64_t v = 0;
         if (inc_mask) {
-            const int first = __ffs(inc_mask) - 1;
-            return prefix + warp_sum_u64(lane <= first ? v : 0ull);
+            const int first_lane = __ffs(inc_mask) - 1;
+#pragma unroll
+            for (int q = 0; q < kLookBackPerLane; ++q) {
+                const bool take = lane < first_lane || (lane == first_lane && q <= first_q);
+                v += take ? (s[q] & kValMask) : 0ull;
+            }
+            return prefix + warp_sum_u64(v);
         }
+#pragma unroll
+        for (int q = 0; q < kLookBackPerLane; ++q) v += s[q] & kValMask;
         prefix += warp_sum_u64(v);
-        p -= 32;
+        base -= 32 * kLookBackPerLane;
     }
 }
 
@@ -358,12 +379,12 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     uint32_t* out_ring = smem + kInRing;
     uint32_t* bitmaps = smem + kInRing + kOutRing;  // 2 x kBitmapSmemWords
     __shared__ __align__(8) uint64_t full[kSlots], empty[kSlots], ofull[kOutQ], oempty[kOutQ];
+    __shared__ __align__(8) uint64_t s_released_out;  // output ring: virtual offset written out so far
+    __shared__ uint32_t s_otile[kOutQ], s_ocount[kOutQ];
+    __shared__ uint64_t s_ostart[kOutQ];
     __shared__ InDesc in_desc[kSlots];
     __shared__ uint64_t s_in_end[kSlots];  // producer-private: ring end of the tile in each slot
-    __shared__ OutDesc out_desc[kOutQ];
-    __shared__ __align__(8) uint64_t s_released_out;
     __shared__ uint32_t s_warp[2][kConsumerWarps];  // by tile parity: a warp may run one tile ahead
-    __shared__ uint32_t s_ooff;
 
     uint32_t* err = reinterpret_cast<uint32_t*>(ws);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -376,7 +397,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
             mbar_init(&empty[i], kConsumerWarps);
         }
         for (int i = 0; i < kOutQ; ++i) {
-            mbar_init(&ofull[i], 1);
+            mbar_init(&ofull[i], kConsumerWarps);  // every consumer warp has written its matches
             mbar_init(&oempty[i], 1);
         }
         s_released_out = 0;
@@ -386,9 +407,13 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
 
     if (warp == kProducerWarp) {
         // ------------------------------------------------------ producer --
-        // This CTA takes groups blockIdx.x, blockIdx.x + gridDim.x, ...; the
-        // split entries of the next group load while the current one stages.
-        // Lane x computes the staging parameters of the group's tile x.
+        // Groups of kGroup consecutive tiles are handed out by a ticket
+        // counter, so groups complete roughly in global order and a
+        // look-back finds an inclusive prefix nearby.  Tickets are fetched
+        // two groups ahead and split entries one group ahead, so neither
+        // latency stalls the staging.  Lane x computes the staging parameters
+        // of the group's tile x.
+        uint32_t* ticket = reinterpret_cast<uint32_t*>(ws + kOffTicket);
         uint64_t head = 0, released = 0;  // virtual ring offsets (lane 0)
         uint32_t k = 0, k_rel = 0;        // tiles staged / tiles known released
         bool done = false;
@@ -405,14 +430,21 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
             ++k_rel;
             return true;
         };
-        uint64_t g = blockIdx.x;
+        uint32_t tk0 = 0, tk1 = 0;
+        if (lane == 0) {
+            tk0 = atomicAdd(ticket, 1u);
+            tk1 = atomicAdd(ticket, 1u);
+        }
+        uint64_t g = __shfl_sync(kFullMask, tk0, 0);
+        uint64_t g_next = __shfl_sync(kFullMask, tk1, 0);
         uint64_t sp_a, sp_b;
         load_splits(g, sp_a, sp_b);
         while (!done) {
             const uint64_t t_first = g * kGroup;
-            const uint64_t gn = g + gridDim.x;
+            uint32_t tk2 = 0;
+            if (lane == 0 && t_first < nTiles) tk2 = atomicAdd(ticket, 1u);  // two groups ahead
             uint64_t nsp_a, nsp_b;
-            load_splits(gn, nsp_a, nsp_b);  // in flight while this group is staged
+            load_splits(g_next, nsp_a, nsp_b);  // in flight while this group is staged
             // ---- lane x: parameters of tile t_first + x ----
             uint64_t a0 = __shfl_sync(kFullMask, sp_a, lane < kGroup ? lane : 0);
             uint64_t a1 = __shfl_sync(kFullMask, sp_a, lane < kGroup ? lane + 1 : 1);
@@ -495,7 +527,8 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
                 if (done) break;
                 ++k;
             }
-            g = gn;
+            g = g_next;
+            g_next = __shfl_sync(kFullMask, tk2, 0);
             sp_a = nsp_a;
             sp_b = nsp_b;
         }
@@ -504,30 +537,32 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
 
     if (warp == kOutputWarp) {
         // -------------------------------------------------------- output --
-        // One look-back per group (its first tile); later tiles of the group
-        // follow from the running prefix.
+        // For each tile this CTA consumed, in order: its exclusive prefix (a
+        // look-back for the first tile of a group, else the running sum), its
+        // inclusive prefix published, its matches copied to global memory.
         if constexpr (kOut) {
             uint64_t prefix = 0;
             for (uint32_t k = 0;; ++k) {
-                const uint32_t j = k % kOutQ, round = k / kOutQ;
-                if (!mbar_wait_bounded(&ofull[j], round & 1, err, 4, k)) break;
-                const OutDesc d = out_desc[j];
-                if (d.tile == kEndTile) break;
-                if (d.tile % kGroup == 0) prefix = d.tile > 0 ? look_back(status, d.tile, err) : 0;
-                if (d.tile > 0 && lane == 0) st_relaxed_u64(status + d.tile, kFlagInc | ((prefix + d.count) & kValMask));
+                const uint32_t q = k % kOutQ;
+                if (!mbar_wait_bounded(&ofull[q], (k / kOutQ) & 1u, err, 4, k)) break;
+                const uint32_t t = s_otile[q], count = s_ocount[q];
+                const uint64_t start = s_ostart[q];
+                if (t == kEndTile) break;
+                if (t % kGroup == 0) prefix = t > 0 ? look_back(status, t, err) : 0;
+                if (t > 0 && lane == 0) st_relaxed_u64(status + t, kFlagInc | ((prefix + count) & kValMask));
                 bool overflow = false;
-                for (uint32_t x = lane; x < d.count; x += 32) {
+                for (uint32_t x = lane; x < count; x += 32) {
                     const uint64_t pos = prefix + x;
-                    if (pos < out_cap) out[pos] = out_ring[d.off + x];
+                    if (pos < out_cap) out[pos] = out_ring[(start + x) & (kOutRing - 1)];
                     else overflow = true;
                 }
-                if (overflow) record_error(err, SI_ERR_OUTPUT_OVERFLOW);
-                prefix += d.count;
-                if (lane == 0 && d.tile + 1 == nTiles) *d_count = prefix;
+                if (overflow) record_error(err, SI_ERR_OUTPUT_OVERFLOW, 9, t);
+                prefix += count;
+                if (lane == 0 && t + 1 == nTiles) *d_count = prefix;
                 __syncwarp();
                 if (lane == 0) {
-                    st_release_shared_u64(&s_released_out, d.end);
-                    mbar_arrive(&oempty[j]);
+                    st_release_shared_u64(&s_released_out, start + count);
+                    mbar_arrive(&oempty[q]);
                 }
             }
         }
@@ -536,10 +571,10 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
 
     // ---------------------------------------------------------- consumers --
     uint64_t my_count = 0;     // count-only: this thread's matches over all its tiles
-    uint64_t ohead = 0;        // thread 0: virtual output-ring head
+    uint64_t ohead = 0;        // element output: virtual output-ring head (same in every thread)
     uint32_t stale0 = 0u, stale1 = 0u;  // bitmap words left set in each buffer
     uint32_t nbm = 0;          // bitmap tiles so far (buffer parity)
-    uint32_t k = 0;            // tiles consumed so far = index of the next output-queue entry
+    uint32_t k = 0;            // tiles consumed so far
     for (;; ++k) {
         const uint32_t slot = k % kSlots;
         if (!mbar_wait_bounded(&full[slot], (k / kSlots) & 1, err, 5, k)) break;
@@ -565,7 +600,6 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
             my_count += cnt;
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[slot]);  // this warp is done with the tile
-            continue;
         } else {
             // block scan over the consumer warps
             const uint32_t incl = warp_inclusive_scan(cnt);
@@ -578,58 +612,55 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
                 wsum += w < warp ? v : 0u;
                 tile_count += v;
             }
-            const uint32_t excl = incl - cnt + wsum;
-            // the tile's aggregate goes out at once, for later tiles' look-backs
-            if (tid == 32) st_relaxed_u64(status + d.tile, (d.tile == 0 ? kFlagInc : kFlagAgg) | tile_count);
+            const uint32_t q = k % kOutQ;
             if (tid == 0) {
-                // same placement rule as the input ring (a skipped tail is free
-                // once every earlier tile has been written out)
-                const uint64_t live_end = ohead;
-                const uint64_t ophys = ohead % kOutRing;
-                if (ophys + tile_count > kOutRing) ohead += kOutRing - ophys;
-                bool space = false;
-                for (WaitBudget budget; !budget.expired();) {
-                    const uint64_t rel = ld_acquire_shared_u64(&s_released_out);
-                    if (rel >= live_end || ohead + tile_count - rel <= kOutRing) {
-                        space = true;
+                // the tile's aggregate goes out at once, for other tiles'
+                // look-backs (before the hand-off below, after which the
+                // output warp overwrites it with the inclusive value)
+                st_relaxed_u64(status + d.tile, (d.tile == 0 ? kFlagInc : kFlagAgg) | tile_count);
+            }
+            // queue entry q and ring space [ohead, ohead + tile_count) must be
+            // free: the output warp has written out what they last held
+            if (lane == 0) mbar_wait_bounded(&oempty[q], ((k / kOutQ) & 1u) ^ 1u, err, 7, k);
+            if (lane == 0 && tile_count) {
+                for (WaitBudget budget;;) {
+                    if (ohead + tile_count - ld_acquire_shared_u64(&s_released_out) <= kOutRing) break;
+                    if (budget.expired()) {
+                        record_error(err, SI_ERR_TIMEOUT, 6, d.tile);
                         break;
                     }
                     __nanosleep(20);
                 }
-                if (!space) record_error(err, SI_ERR_TIMEOUT, 6, d.tile);
-                s_ooff = space ? static_cast<uint32_t>(ohead % kOutRing) : kEndTile;
-                ohead += tile_count;
             }
-            named_barrier(kConsumerBar, kConsumers);
-            const uint32_t ooff = s_ooff;
-            if (ooff == kEndTile) break;  // gave up waiting for output space (error recorded)
-            uint32_t m = tm.mask, c = excl;
+            __syncwarp();
+            uint32_t m = tm.mask;
+            uint64_t pos = ohead + incl - cnt + wsum;
             while (m) {
                 const int x = __ffs(m) - 1;
                 m &= m - 1;
-                out_ring[ooff + c++] = tm.src[tm.start + x];
+                out_ring[pos++ & (kOutRing - 1)] = tm.src[tm.start + x];
             }
-            named_barrier(kConsumerBar, kConsumers);  // all matches written, tile no longer read
-            if (lane == 0) mbar_arrive(&empty[slot]);
             if (tid == 0) {
-                const uint32_t q = k % kOutQ;
-                mbar_wait_bounded(&oempty[q], ((k / kOutQ) & 1) ^ 1, err, 7, k);
-                OutDesc& od = out_desc[q];
-                od.tile = d.tile;
-                od.off = ooff;
-                od.count = tile_count;
-                od.end = ohead;
-                mbar_arrive(&ofull[q]);
+                s_otile[q] = d.tile;
+                s_ocount[q] = tile_count;
+                s_ostart[q] = ohead;
+            }
+            ohead += tile_count;
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&empty[slot]);  // this warp is done with the input tile
+                mbar_arrive(&ofull[q]);     // ... and has written its matches
             }
         }
     }
     if constexpr (kOut) {
-        if (tid == 0) {  // end marker for the output warp
+        if (tid == 0) {  // end marker for the output warp (its own phase of entry q)
             const uint32_t q = k % kOutQ;
-            if (mbar_wait_bounded(&oempty[q], ((k / kOutQ) & 1) ^ 1, err, 8, k)) {
-                out_desc[q].tile = kEndTile;
-                mbar_arrive(&ofull[q]);
-            }
+            mbar_wait_bounded(&oempty[q], ((k / kOutQ) & 1u) ^ 1u, err, 8, k);
+            s_otile[q] = kEndTile;
+            s_ocount[q] = 0;
+            s_ostart[q] = ohead;
+            for (int w = 0; w < kConsumerWarps; ++w) mbar_arrive(&ofull[q]);
         }
     } else {
         const uint64_t wsum = warp_sum_u64(my_count);
