@@ -117,12 +117,35 @@ si_status si_workspace_diagnostic(const void* d_workspace, si_stream_t stream, u
  * to d_flag (device uint32).  No workspace. */
 si_status si_validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, si_stream_t stream);
 
+/* --------------------------------------------------- MISI, dense form --
+ * All pairs a < b of a collection of k sets over values 0..universe:
+ * counts[tri(k, a, b)] = |S_a ∩ S_b|, tri = include/util.hpp:68-70 (the
+ * reference's single-run result order, src/bitmap_naive.cu:443-447).
+ *
+ * d_elements / d_offsets: the collection in CSR form on the device (set a is
+ * d_elements[d_offsets[a] .. d_offsets[a+1]), k + 1 offsets).
+ * t = SI_TECH_MM: tensor-core product of the 0/1 incidence matrix, dtype
+ *     INT8 (s32 accumulation) or FP8-e4m3 (f32 accumulation), both exact.
+ *     Replaces the mm tile loop, src/matrix_multiplication.cu:139-184
+ *     (host-built FP32 matrix + cublasSgemm per tile pair).
+ * t = SI_TECH_BITMAP_NAIVE: bitmaps + AND-popcount on CUDA cores, the plain
+ *     comparison.  Replaces src/bitmap_naive.cu:433-441 (generateBitmaps +
+ *     intersectPerPair).
+ * d_counts: device uint32[k*(k-1)/2].
+ */
+typedef enum si_dense_dtype { SI_DENSE_INT8 = 0, SI_DENSE_FP8_E4M3 = 1 } si_dense_dtype;
+size_t si_misi_dense_workspace_size(uint32_t k, uint32_t universe, si_technique t);
+si_status si_misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint32_t universe,
+                        si_technique t, si_dense_dtype dtype, uint32_t* d_counts, void* d_workspace,
+                        size_t workspace_bytes, si_stream_t stream);
+
 /* ---------------------------------------------------------- phase timer --
  * Named cudaEvent pairs around the engine's own kernel launches, recorded on
  * the launching stream while enabled -- the counterpart of the reference's
  * DeviceTimer (include/device_timer.cuh:20-78), which wraps every phase of
- * every executable the same way.  Phase names of the single-pair pipeline:
- * "sisi_prepare", "sisi_split", "sisi_tile".  si_timer_read synchronises on
+ * every executable the same way.  Phase names: single pair "sisi_prepare",
+ * "sisi_split", "sisi_tile"; dense all pairs "mm_incidence", "mm_gemm",
+ * "naive_bitmaps", "naive_popcount".  si_timer_read synchronises on
  * the recorded events and returns the summed milliseconds and the number of
  * launches of one phase.
  */
@@ -139,6 +162,13 @@ si_status si_timer_read(const char* phase, double* total_ms, uint64_t* launches)
  * [lo, hi), written ascending to out[n].  hi - lo <= 2^32.
  */
 si_status si_gen_uniform(uint64_t seed, uint64_t n, uint64_t lo, uint64_t hi, uint32_t* out, int threads);
+
+/* si_gen_bernoulli: k sets over values [0, n_values), value v in set a with
+ * probability p, independently.  Call once with elements == NULL to fill
+ * offsets[k + 1] (CSR offsets), then again with elements[offsets[k]] and the
+ * same offsets to fill the sets (each ascending). */
+si_status si_gen_bernoulli(uint64_t seed, uint32_t k, uint32_t n_values, double p, uint64_t* offsets,
+                           uint32_t* elements, int threads);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,9 @@ _SIGNATURES = {
     "si_workspace_diagnostic": (_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     "si_validate_sorted": (_int, [_vp, _u64, _vp, _vp]),
     "si_gen_uniform": (_int, [_u64, _u64, _u64, _u64, _vp, _int]),
+    "si_gen_bernoulli": (_int, [_u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, _vp, _vp, _int]),
+    "si_misi_dense_workspace_size": (_sz, [ctypes.c_uint32, ctypes.c_uint32, _int]),
+    "si_misi_dense": (_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _int, _int, _vp, _vp, _sz, _vp]),
     "si_timer_enable": (None, [_int]),
     "si_timer_reset": (None, []),
     "si_timer_read": (_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_u64)]),

@@ -153,6 +153,44 @@ def intersect_host(a_host: torch.Tensor, b_host: torch.Tensor, tech="ip", out_ho
     return c, out_host[:c]
 
 
+class Collection:
+    """A collection of sorted sets in CSR form on the device (the reference's
+    Dataset after its cudaMemcpy + offset scan, e.g. src/ip.cu:129-137)."""
+
+    def __init__(self, elements: torch.Tensor, offsets: torch.Tensor, universe: int):
+        if offsets.dtype != torch.int64 or not offsets.is_cuda or not elements.is_cuda:
+            raise ValueError("offsets must be an int64 CUDA tensor and elements a CUDA tensor")
+        _check_set(elements, "elements")
+        self.elements, self.offsets, self.universe = elements, offsets, int(universe)
+        self.k = offsets.numel() - 1
+
+    @classmethod
+    def from_dataset(cls, ds, device="cuda"):
+        import numpy as np
+        el = torch.from_numpy(np.ascontiguousarray(ds.elements, dtype=np.uint32).view(np.int32)).to(device)
+        off = torch.from_numpy(ds.offsets.astype(np.int64)).to(device)
+        return cls(el, off, ds.universe)
+
+
+DENSE_DTYPES = {"int8": 0, "fp8": 1, "fp8_e4m3": 1}
+
+
+def misi_dense(col: Collection, tech="mm", dtype="int8", workspace: Workspace | None = None, stream=None,
+               check_errors: bool = True) -> torch.Tensor:
+    """uint32 counts (as int32 storage) of every pair a < b, triangular order."""
+    t = technique(tech)
+    k = col.k
+    ws = workspace or Workspace(col.elements.device)
+    buf = ws.get(lib.si_misi_dense_workspace_size(k, col.universe, int(t)))
+    counts = torch.empty(max(1, k * (k - 1) // 2), dtype=torch.int32, device=col.elements.device)
+    st = lib.si_misi_dense(_ptr(col.elements), _ptr(col.offsets), k, col.universe, int(t), DENSE_DTYPES[dtype],
+                           _ptr(counts), _ptr(buf), buf.numel(), _stream(stream))
+    check(st, "si_misi_dense")
+    if check_errors:
+        ws.check(stream)
+    return counts[: k * (k - 1) // 2]
+
+
 def validate_sorted(x: torch.Tensor, stream=None) -> bool:
     _check_set(x, "x")
     flag = torch.zeros(1, dtype=torch.int32, device=x.device)
@@ -164,6 +202,7 @@ def status_string(s: int) -> str:
     return lib.si_status_string(int(s)).decode()
 
 
-__all__ = ["Status", "Technique", "Workspace", "HostPair", "intersect", "intersect_host", "sisi_into",
+__all__ = ["Status", "Technique", "Workspace", "HostPair", "Collection", "misi_dense", "intersect", "intersect_host",
+           "sisi_into",
            "sisi_workspace_size",
            "technique", "validate_sorted", "status_string"]

@@ -159,6 +159,25 @@ si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
     }
 }
 
+size_t si_misi_dense_workspace_size(uint32_t k, uint32_t universe, si_technique t) {
+    if (t != SI_TECH_MM && t != SI_TECH_BITMAP_NAIVE) return 0;
+    return si::dense_workspace_size(k, universe, t);
+}
+
+si_status si_misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint32_t universe,
+                        si_technique t, si_dense_dtype dtype, uint32_t* d_counts, void* d_workspace,
+                        size_t workspace_bytes, si_stream_t stream) {
+    if (t != SI_TECH_MM && t != SI_TECH_BITMAP_NAIVE) return SI_ERR_UNSUPPORTED;
+    if (dtype != SI_DENSE_INT8 && dtype != SI_DENSE_FP8_E4M3) return SI_ERR_INVALID_ARGUMENT;
+    if (!d_offsets || !d_workspace || (k >= 2 && !d_counts)) return SI_ERR_INVALID_ARGUMENT;
+    if (!si::aligned(d_elements, 4) || !si::aligned(d_offsets, 8) || !si::aligned(d_counts, 4) ||
+        !si::aligned(d_workspace, 256))
+        return SI_ERR_INVALID_ARGUMENT;
+    if (universe >= (1u << 24)) return SI_ERR_UNSUPPORTED;  // counts must stay exact in f32
+    return si::misi_dense(d_elements, d_offsets, k, universe, t, dtype == SI_DENSE_FP8_E4M3, d_counts,
+                          d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
 si_status si_workspace_check(const void* d_workspace, si_stream_t stream) {
     if (!d_workspace) return SI_ERR_INVALID_ARGUMENT;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

@@ -11,6 +11,9 @@
 //  * sparse case: sequential draws from a splitmix64 stream, rejecting
 //    repeats until n distinct values are held, then sorted (the classic
 //    draw-until-distinct construction of a uniform n-subset).
+//
+// Bernoulli membership (a dense collection): value v is in set a iff
+// hash32(seed, a * 2^32 + v) < p * 2^32, independently for every (a, v).
 #include <algorithm>
 #include <cstdint>
 #include <thread>
@@ -135,6 +138,34 @@ void uniform_sparse(uint64_t seed, uint64_t n, uint64_t lo, uint64_t U, uint32_t
 
 }  // namespace
 }  // namespace si
+
+extern "C" si_status si_gen_bernoulli(uint64_t seed, uint32_t k, uint32_t n_values, double p, uint64_t* offsets,
+                                      uint32_t* elements, int threads) {
+    if (!offsets || !(p >= 0.0 && p <= 1.0)) return SI_ERR_INVALID_ARGUMENT;
+    const uint64_t thr = static_cast<uint64_t>(p * 4294967296.0);  // member iff hash < thr
+    const int T = si::resolve_threads(threads);
+    auto member = [&](uint64_t a, uint64_t v) { return si::hash32(seed, (a << 32) | v) < thr; };
+    if (!elements) {
+        offsets[0] = 0;
+        si::parallel_chunks(k, T, [&](int, uint64_t b, uint64_t e) {
+            for (uint64_t a = b; a < e; ++a) {
+                uint64_t c = 0;
+                for (uint64_t v = 0; v < n_values; ++v) c += member(a, v);
+                offsets[a + 1] = c;
+            }
+        });
+        for (uint32_t a = 0; a < k; ++a) offsets[a + 1] += offsets[a];
+        return SI_OK;
+    }
+    si::parallel_chunks(k, T, [&](int, uint64_t b, uint64_t e) {
+        for (uint64_t a = b; a < e; ++a) {
+            uint64_t x = offsets[a];
+            for (uint64_t v = 0; v < n_values; ++v)
+                if (member(a, v)) elements[x++] = static_cast<uint32_t>(v);
+        }
+    });
+    return SI_OK;
+}
 
 extern "C" si_status si_gen_uniform(uint64_t seed, uint64_t n, uint64_t lo, uint64_t hi, uint32_t* out, int threads) {
     if (hi < lo || hi - lo > (1ull << 32) || hi > (1ull << 32) || n > hi - lo || (n && !out))

@@ -50,6 +50,13 @@ size_t ip_workspace_size(uint64_t nA, uint64_t nB);
 si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
                   uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream, int inner = 0);
 
+// ---- all pairs of a dense collection (si_misi_dense.cu) ----
+// t: SI_TECH_MM (tensor cores; fp8 selects FP8-e4m3 operands instead of INT8)
+// or SI_TECH_BITMAP_NAIVE (plain AND-popcount on CUDA cores).
+size_t dense_workspace_size(uint32_t k, uint32_t universe, si_technique t);
+si_status misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint32_t universe,
+                     si_technique t, int fp8, uint32_t* d_counts, void* ws, size_t ws_bytes, cudaStream_t stream);
+
 // ---- sortedness check (si_api.cu) ----
 si_status validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, cudaStream_t stream);
 

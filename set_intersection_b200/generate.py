@@ -52,3 +52,22 @@ def sisi_skewed(seed: int = 5, n_small: int = 1 << 16, n_large: int = 1 << 26,
     b[pos_p] = planted
     b[mask] = rest.astype(np.uint32)
     return a, b
+
+
+def bernoulli(seed: int, k: int, n_values: int, p: float, threads: int = 0):
+    """k sets over [0, n_values), each value a member with probability p.
+    Returns (elements uint32, offsets int64[k + 1]) in CSR form."""
+    offsets = np.empty(k + 1, dtype=np.uint64)
+    st = lib.si_gen_bernoulli(seed, k, n_values, p, offsets.ctypes.data_as(ctypes.c_void_p), None, threads)
+    check(st, "si_gen_bernoulli")
+    elements = np.empty(int(offsets[-1]), dtype=np.uint32)
+    st = lib.si_gen_bernoulli(seed, k, n_values, p, offsets.ctypes.data_as(ctypes.c_void_p),
+                              elements.ctypes.data_as(ctypes.c_void_p), threads)
+    check(st, "si_gen_bernoulli")
+    return elements, offsets.astype(np.int64)
+
+
+def misi_dense(seed: int = 6, k: int = 16384, n_values: int = 65536, p: float = 0.05):
+    """The dense all-pairs collection: 16384 sets over 65536 values,
+    Bernoulli(0.05) membership."""
+    return bernoulli(seed, k, n_values, p)

@@ -58,6 +58,46 @@ def test_invalid_arguments_rejected_on_host():
     assert L.si_workspace_check(nul, nul) == Status.INVALID_ARGUMENT
 
 
+def test_dense_invalid_arguments_rejected_on_host():
+    L = si.lib
+    nul = ctypes.c_void_p(None)
+    fake = ctypes.c_void_p(0x1000)
+    mm, naive = int(Technique.MM), int(Technique.BITMAP_NAIVE)
+    assert L.si_misi_dense(fake, fake, 10, 100, int(Technique.IP), 0, fake, fake, 1 << 20, nul) == Status.UNSUPPORTED
+    assert L.si_misi_dense(fake, fake, 10, 100, mm, 2, fake, fake, 1 << 20, nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi_dense(fake, nul, 10, 100, mm, 0, fake, fake, 1 << 20, nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi_dense(fake, fake, 10, 100, mm, 0, nul, fake, 1 << 20, nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi_dense(fake, fake, 10, 100, mm, 0, fake, ctypes.c_void_p(0x1010), 1 << 20,
+                           nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi_dense(fake, fake, 10, 1 << 24, mm, 0, fake, fake, 1 << 40, nul) == Status.UNSUPPORTED
+    for t in (mm, naive):
+        need = L.si_misi_dense_workspace_size(16384, 65535, t)
+        assert L.si_misi_dense(fake, fake, 16384, 65535, t, 0, fake, fake, need - 1, nul) == \
+            Status.WORKSPACE_TOO_SMALL
+    # tensor-core operand: one byte per (set, value), rows padded to 256, values to 128
+    assert L.si_misi_dense_workspace_size(16384, 65535, mm) == 256 + 16384 * 65536
+    assert L.si_misi_dense_workspace_size(300, 200, mm) == 256 + 512 * 256
+    # plain bitmaps: one bit per (set, value)
+    assert L.si_misi_dense_workspace_size(16384, 65535, naive) == 256 + 16384 * 65536 // 8
+    assert L.si_misi_dense_workspace_size(10, 100, int(Technique.IP)) == 0
+
+
+def test_bernoulli_generator_density_and_determinism():
+    from set_intersection_b200 import generate
+    el, off = generate.bernoulli(9, 300, 4000, 0.05, threads=3)
+    el2, off2 = generate.bernoulli(9, 300, 4000, 0.05, threads=11)
+    assert np.array_equal(el, el2) and np.array_equal(off, off2)
+    assert off[0] == 0 and np.all(np.diff(off) >= 0) and off[-1] == el.size
+    assert abs(el.size / (300 * 4000) - 0.05) < 0.005
+    for a in range(300):
+        s = el[off[a]:off[a + 1]]
+        assert np.all(np.diff(s.astype(np.int64)) > 0) and (s.size == 0 or s[-1] < 4000)
+    full_el, full_off = generate.bernoulli(1, 3, 50, 1.0)
+    assert np.array_equal(full_el, np.tile(np.arange(50, dtype=np.uint32), 3))
+    empty_el, empty_off = generate.bernoulli(1, 3, 50, 0.0)
+    assert empty_el.size == 0 and np.all(empty_off == 0)
+
+
 def test_workspace_size_grows_with_input():
     f = si.lib.si_sisi_workspace_size
     small = f(1000, 1000, int(Technique.IP))
