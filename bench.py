@@ -41,6 +41,7 @@ sys.path.insert(0, ROOT)
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
 CACHE_DIR = os.environ.get("SI_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "si_bench_cache"))
 
 WORKLOADS = {
@@ -53,6 +54,11 @@ WORKLOADS = {
                        n=1 << 20, universe=1 << 24, seeds=(1, 2)),
     "sisi_skewed": dict(desc="SISI |A|=2^16, |B|=2^26 from [0,2^30), 20% of A planted into B, seed 5",
                         n=None, universe=1 << 30, seeds=(5,)),
+    "misi_dense": dict(desc="MISI all pairs: 16384 sets over values [0,65536), Bernoulli(0.05) membership, seed 6",
+                       k=16384, n_values=65536, p=0.05, seeds=(6,)),
+    "misi_dense_small": dict(desc="MISI all pairs: 4096 sets over values [0,65536), Bernoulli(0.05), seed 6 "
+                                  "(incidence 256 MiB > L2; profiling size)",
+                             k=4096, n_values=65536, p=0.05, seeds=(6,)),
 }
 
 
@@ -374,6 +380,246 @@ def run_ours(args, rank: int, world: int):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------- MISI, dense form --
+def dense_collection(name: str):
+    from set_intersection_b200 import generate
+    w = WORKLOADS[name]
+    return generate.bernoulli(w["seeds"][0], w["k"], w["n_values"], w["p"])
+
+
+def dense_sample(name: str, k_sample: int):
+    """The first k_sample sets of the workload (same density and universe)."""
+    from set_intersection_b200 import generate
+    w = WORKLOADS[name]
+    return generate.bernoulli(w["seeds"][0], k_sample, w["n_values"], w["p"])
+
+
+def dense_reference_ms(el, off, n_values: int, tmpdir: str, threads: int) -> float:
+    """One run of the reference's boost_bitset executable (all pairs, OpenMP)
+    on a dataset file; its own HostTimer figure for the intersection phase."""
+    import oracle
+    from set_intersection_b200 import dataset as fmt
+    path = os.path.join(tmpdir, "dense.bin")
+    if not os.path.exists(path):
+        sizes = np.diff(off).astype(np.uint32)
+        fmt.write_dataset(path, fmt.Dataset(len(sizes), n_values - 1, sizes, el))
+    r = oracle.run_ref("boost_bitset", path, threads=threads)
+    return r["host_ms"]["Boost bitset intersection"]
+
+
+def dense_port_ms(el, off, n_values: int, threads: int) -> float:
+    import oracle
+    k = off.size - 1
+    t0 = time.perf_counter()
+    oracle.all_pairs(el, off, k, n_values - 1, "bitset", threads=threads)
+    return (time.perf_counter() - t0) * 1e3
+
+
+def dense_cpu_measure(name: str, k_sample: int, steps: int, warmup: int):
+    import oracle
+    el, off = dense_sample(name, k_sample)
+    n_values = WORKLOADS[name]["n_values"]
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_binary("boost_bitset") else "port"
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        for i in range(warmup + steps):
+            ms = (dense_reference_ms(el, off, n_values, td, threads) if kind == "reference"
+                  else dense_port_ms(el, off, n_values, threads))
+            if i >= warmup:
+                times.append(ms)
+    ms = statistics.median(times)
+    pairs = k_sample * (k_sample - 1) // 2
+    desc = (f"first {k_sample} sets of the workload ({pairs} pairs), boost_bitset --threads {threads} "
+            f"(src/boost_bitset.cpp:60-84), median of {steps} runs timed by its HostTimer")
+    return kind, threads, pairs / (ms * 1e-3), desc, ms
+
+
+def run_reference_dense(args, rank: int):
+    if rank != 0:
+        return
+    kind, threads, value, desc, ms = dense_cpu_measure(args.workload, 1024, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": "MISI pairs/s", "value": value, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "technique": "boost_bitset"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind, "sample": desc},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours_dense(args, rank: int, world: int):
+    import ctypes
+    import torch
+    from set_intersection_b200 import api
+    from set_intersection_b200._lib import lib
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        dist.init_process_group("nccl", device_id=dev)
+    tech = args.technique if args.technique in ("mm", "bitmap_naive") else "mm"
+    dtype = args.dtype
+    w = WORKLOADS[args.workload]
+    el, off = dense_collection(args.workload)
+    k, universe = off.size - 1, w["n_values"] - 1
+    pairs = k * (k - 1) // 2
+    stream = torch.cuda.Stream(dev)
+    col = api.Collection(torch.from_numpy(el.view(np.int32)).to(dev), torch.from_numpy(off).to(dev), universe)
+    ws = api.Workspace(dev)
+    counts = torch.empty(pairs, dtype=torch.int32, device=dev)
+
+    def step(t=tech, d=dtype, out=counts):
+        api.misi_dense_into(col, out, t, d, ws, stream)
+
+    # parity of the benchmarked call, once, before timing: against the plain
+    # popcount kernel on every pair and the oracle on sampled pairs
+    step()
+    ws.check(stream)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        import oracle
+        plain = torch.empty_like(counts)
+        api.misi_dense_into(col, plain, "bitmap_naive", "int8", ws, stream)
+        ws.check(stream)
+        same = bool(torch.equal(plain, counts))
+        rng = np.random.default_rng(1)
+        a = rng.integers(0, k - 1, 20000)
+        b = a + 1 + (rng.random(20000) * (k - 1 - a)).astype(np.int64)
+        want = oracle.pairs(el, off, k, np.stack([a, b], 1))
+        idx = pairs - (k - a) * (k - a - 1) // 2 + b - a - 1
+        got = counts.cpu().numpy().view(np.uint32)[idx]
+        parity = same and bool(np.array_equal(got, want))
+        log(f"parity: all pairs vs plain kernel {same}, 20000 sampled pairs vs oracle {np.array_equal(got, want)}")
+        del plain
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    gemm_phase = b"mm_gemm" if tech == "mm" else b"naive_popcount"
+    lib.si_timer_reset()
+    lib.si_timer_enable(1)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        stop.record(stream)
+        stop.synchronize()
+    lib.si_timer_enable(0)
+    ms_total = start.elapsed_time(stop)
+    k_ms, k_n = ctypes.c_double(0), ctypes.c_uint64(0)
+    lib.si_timer_read(gemm_phase, ctypes.byref(k_ms), ctypes.byref(k_n))
+    lib.si_timer_reset()
+    ws.check(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * pairs / (ms_step * 1e-3)
+
+    # the plain AND-popcount kernel on the same GPU, for the speed-up
+    plain_ms = None
+    if tech == "mm" and not args.no_plain:
+        step(t="bitmap_naive", d="int8")
+        stream.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n_plain = max(1, min(3, args.steps))
+        p0.record(stream)
+        for _ in range(n_plain):
+            step(t="bitmap_naive", d="int8")
+        p1.record(stream)
+        p1.synchronize()
+        plain_ms = p0.elapsed_time(p1) / n_plain
+
+    e2e = None
+    if not args.no_e2e:
+        h_el = torch.from_numpy(el.view(np.int32)).pin_memory()
+        h_off = torch.from_numpy(off).pin_memory()
+        h_counts = torch.empty(pairs, dtype=torch.int32).pin_memory()
+        ctx = api.HostCollection(dev)
+        api.misi_dense_host(h_el, h_off, universe, tech, dtype, h_counts, ctx, stream)
+        e_steps = max(1, min(args.steps, args.e2e_steps))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e_steps):
+            api.misi_dense_host(h_el, h_off, universe, tech, dtype, h_counts, ctx, stream)
+        e1.record(stream)
+        e1.synchronize()
+        e_ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e_step = e_ms / e_steps
+        e2e = {"value": world * pairs / (e_step * 1e-3), "unit": "pairs/s",
+               "h2d_bytes_per_step": int(4 * el.size + 8 * off.size), "d2h_bytes_per_step": int(4 * pairs),
+               "ms_per_step": e_step, "steps": e_steps}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    avg_ms = k_ms.value / max(1, k_n.value)
+    if tech == "mm":
+        # algorithmic work: one multiply-add per (pair a < b, value)
+        ops = 2.0 * pairs * w["n_values"]
+        bf16 = peaks.get("bf16_tflops", FALLBACK_BF16_TFLOPS)
+        peak = 2.0 * bf16
+        achieved = ops / (avg_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "kernel": f"tc_gemm_kernel<{dtype}>", "alg_ops_per_launch": ops,
+                "avg_launch_ms": avg_ms, "launches": int(k_n.value),
+                "peak_source": ("2 x measured dense bf16 (8-bit operands run at twice the 16-bit rate)"
+                                if "bf16_tflops" in peaks else "2 x fallback bf16")}
+    else:
+        roof = {"bound": "alu", "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None,
+                "kernel": "popcount_gemm_kernel", "avg_launch_ms": avg_ms, "launches": int(k_n.value)}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        kind, threads, cval, desc, _ = dense_cpu_measure(args.workload, 1024, steps=3, warmup=1)
+        cpu = {"value": cval, "unit": "pairs/s", "cores": threads, "kind": kind, "sample": desc}
+
+    line = {
+        "metric": "MISI pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8" if dtype == "int8" else "e4m3",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"], "technique": tech, "operand": dtype,
+                   "k": k, "values": w["n_values"], "pairs": pairs, "elements": int(el.size),
+                   "l2": f"incidence operand {w['k'] * w['n_values'] >> 20} MiB per step > 126 MB L2; no flush",
+                   "parallelism": f"replicas{world}", "parity_vs_oracle": parity,
+                   "plain_popcount_ms_per_step": plain_ms,
+                   "speedup_vs_plain": (plain_ms / ms_step) if plain_ms else None},
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -387,15 +633,18 @@ def main():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-parity", action="store_true")
+    p.add_argument("--no-plain", action="store_true", help="dense: skip timing the plain popcount kernel")
+    p.add_argument("--dtype", choices=["int8", "fp8"], default="int8", help="dense: tensor-core operand type")
     args = p.parse_args()
     if args.warmup < 3:
         p.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
+    dense = args.workload.startswith("misi_dense")
     if args.impl == "reference":
-        run_reference_arm(args, rank)
+        (run_reference_dense if dense else run_reference_arm)(args, rank)
     else:
-        run_ours(args, rank, world)
+        (run_ours_dense if dense else run_ours)(args, rank, world)
 
 
 if __name__ == "__main__":

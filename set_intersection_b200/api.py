@@ -175,20 +175,74 @@ class Collection:
 DENSE_DTYPES = {"int8": 0, "fp8": 1, "fp8_e4m3": 1}
 
 
-def misi_dense(col: Collection, tech="mm", dtype="int8", workspace: Workspace | None = None, stream=None,
-               check_errors: bool = True) -> torch.Tensor:
-    """uint32 counts (as int32 storage) of every pair a < b, triangular order."""
+def n_pairs(k: int) -> int:
+    return k * (k - 1) // 2
+
+
+def misi_dense_into(col: Collection, counts: torch.Tensor, tech="mm", dtype="int8",
+                    workspace: Workspace | None = None, stream=None) -> None:
+    """Asynchronous all-pairs call: counts[tri(k, a, b)] <- |S_a ∩ S_b| for
+    every a < b (counts: int32/uint32 storage, >= k(k-1)/2 elements)."""
     t = technique(tech)
     k = col.k
-    ws = workspace or Workspace(col.elements.device)
+    if counts.numel() < n_pairs(k) or not counts.is_cuda:
+        raise ValueError("counts must be a CUDA tensor of k(k-1)/2 elements")
+    ws = workspace if workspace is not None else Workspace(col.elements.device)
     buf = ws.get(lib.si_misi_dense_workspace_size(k, col.universe, int(t)))
-    counts = torch.empty(max(1, k * (k - 1) // 2), dtype=torch.int32, device=col.elements.device)
     st = lib.si_misi_dense(_ptr(col.elements), _ptr(col.offsets), k, col.universe, int(t), DENSE_DTYPES[dtype],
                            _ptr(counts), _ptr(buf), buf.numel(), _stream(stream))
     check(st, "si_misi_dense")
+
+
+def misi_dense(col: Collection, tech="mm", dtype="int8", workspace: Workspace | None = None, stream=None,
+               check_errors: bool = True) -> torch.Tensor:
+    """uint32 counts (as int32 storage) of every pair a < b, triangular order."""
+    ws = workspace or Workspace(col.elements.device)
+    counts = torch.empty(max(1, n_pairs(col.k)), dtype=torch.int32, device=col.elements.device)
+    misi_dense_into(col, counts, tech, dtype, ws, stream)
     if check_errors:
         ws.check(stream)
-    return counts[: k * (k - 1) // 2]
+    return counts[: n_pairs(col.k)]
+
+
+class HostCollection:
+    """Device buffers and workspace reused by misi_dense_host across calls."""
+
+    def __init__(self, device=None):
+        self.device = torch.device(device if device is not None else "cuda")
+        self.ws = Workspace(self.device)
+        self.el = self.off = self.counts = None
+
+    def _fit(self, buf, n, dtype):
+        if buf is None or buf.numel() < n:
+            buf = torch.empty(max(n, 1), dtype=dtype, device=self.device)
+        return buf
+
+
+def misi_dense_host(elements_host: torch.Tensor, offsets_host: torch.Tensor, universe: int, tech="mm",
+                    dtype="int8", counts_host: torch.Tensor | None = None, ctx: HostCollection | None = None,
+                    stream=None) -> torch.Tensor:
+    """End-to-end all pairs from a HOST collection (CSR: int32/uint32
+    elements, int64 offsets[k+1], pinned for asynchronous copies): copies it to
+    the device, counts every pair, copies the counts back into counts_host
+    (pinned int32[k(k-1)/2]) and returns them."""
+    ctx = ctx or HostCollection()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    k = offsets_host.numel() - 1
+    n = elements_host.numel()
+    ctx.el = ctx._fit(ctx.el, n, torch.int32)
+    ctx.off = ctx._fit(ctx.off, k + 1, torch.int64)
+    ctx.counts = ctx._fit(ctx.counts, n_pairs(k), torch.int32)
+    if counts_host is None:
+        counts_host = torch.empty(max(1, n_pairs(k)), dtype=torch.int32).pin_memory()
+    with torch.cuda.stream(s):
+        ctx.el[:n].copy_(elements_host.view(torch.int32), non_blocking=True)
+        ctx.off[:k + 1].copy_(offsets_host, non_blocking=True)
+        col = Collection(ctx.el[:n], ctx.off[:k + 1], universe)
+        misi_dense_into(col, ctx.counts, tech, dtype, ctx.ws, s)
+        counts_host[:n_pairs(k)].copy_(ctx.counts[:n_pairs(k)], non_blocking=True)
+    ctx.ws.check(s)
+    return counts_host[:n_pairs(k)]
 
 
 def validate_sorted(x: torch.Tensor, stream=None) -> bool:
@@ -202,7 +256,8 @@ def status_string(s: int) -> str:
     return lib.si_status_string(int(s)).decode()
 
 
-__all__ = ["Status", "Technique", "Workspace", "HostPair", "Collection", "misi_dense", "intersect", "intersect_host",
+__all__ = ["Status", "Technique", "Workspace", "HostPair", "Collection", "HostCollection", "misi_dense", "misi_dense_into",
+           "misi_dense_host", "intersect", "intersect_host",
            "sisi_into",
            "sisi_workspace_size",
            "technique", "validate_sorted", "status_string"]
