@@ -74,6 +74,12 @@ const char* si_last_error_string(void);
  * count; element output is this engine's addition, ordered as
  * std::set_intersection orders it.
  *
+ * Techniques: IP merges, HI hashes and BITMAP bit-tests the two sets tile by
+ * tile (value-pivot tiles of <= 4096 elements per set, both sets streamed
+ * once); OBS searches every element of the smaller set in the larger one
+ * (cached top levels in shared memory); AUTO takes OBS when one set is more
+ * than 64 times larger than the other, else BITMAP.
+ *
  * d_count: device uint64, receives |A ∩ B|.
  * d_out:   device uint32[out_cap] or NULL (count only).  When non-NULL,
  *          out_cap must be >= min(nA, nB).

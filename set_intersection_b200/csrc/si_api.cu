@@ -128,9 +128,13 @@ const char* si_last_error_string(void) { return si::g_last_error.c_str(); }
 size_t si_sisi_workspace_size(uint64_t nA, uint64_t nB, si_technique t) {
     switch (t) {
         case SI_TECH_IP:
+        case SI_TECH_HI:
         case SI_TECH_BITMAP:
-        case SI_TECH_AUTO:
             return si::ip_workspace_size(nA, nB);
+        case SI_TECH_AUTO:
+            return std::max(si::ip_workspace_size(nA, nB), si::obs_workspace_size(nA, nB));
+        case SI_TECH_OBS:
+            return si::obs_workspace_size(nA, nB);
         default:
             return 0;
     }
@@ -148,12 +152,18 @@ si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
     switch (t) {
         case SI_TECH_IP:
             return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, d_workspace, workspace_bytes, s, 0);
-        case SI_TECH_BITMAP:
         case SI_TECH_AUTO:
+            // skewed pairs: search the small set in the large one (reads a
+            // fraction of the large set); otherwise stream both through tiles
+            if (std::min(nA, nB) * si::kSkewRatio < std::max(nA, nB))
+                return si::obs_sisi(dA, nA, dB, nB, d_count, d_out, d_workspace, workspace_bytes, s);
             return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, d_workspace, workspace_bytes, s, 1);
-        case SI_TECH_OBS:
+        case SI_TECH_BITMAP:
+            return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, d_workspace, workspace_bytes, s, 1);
         case SI_TECH_HI:
-            return SI_ERR_UNSUPPORTED;
+            return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, d_workspace, workspace_bytes, s, 2);
+        case SI_TECH_OBS:
+            return si::obs_sisi(dA, nA, dB, nB, d_count, d_out, d_workspace, workspace_bytes, s);
         default:
             return SI_ERR_INVALID_ARGUMENT;
     }

@@ -45,8 +45,15 @@ private:
 };
 
 // ---- single-pair tile pipeline (si_sisi_ip.cu) ----
-// inner: 0 = merge path (technique ip), 1 = bitmap probe (technique bitmap).
+// inner: 0 = merge path (technique ip), 1 = bitmap probe (technique bitmap),
+// 2 = hash probe (technique hi).
 size_t ip_workspace_size(uint64_t nA, uint64_t nB);
+// SI_TECH_AUTO searches the smaller set in the larger (obs) when the sizes
+// differ by more than this factor.
+constexpr uint64_t kSkewRatio = 64;
+size_t obs_workspace_size(uint64_t nA, uint64_t nB);
+si_status obs_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
+                   uint32_t* d_out, void* ws, size_t ws_bytes, cudaStream_t stream);
 si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
                   uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream, int inner = 0);
 

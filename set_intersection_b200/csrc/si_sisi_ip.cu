@@ -187,7 +187,11 @@ constexpr int kGroup = 4;                    // consecutive tiles per scheduling
 constexpr uint32_t kInRing = 14336;          // u32: 56 KiB
 constexpr uint32_t kOutRing = 4096;          // u32: 16 KiB, a power of two
 constexpr uint32_t kBitmapSmemWords = 2048;  // u32 per bitmap buffer (8 KiB); two buffers
-constexpr size_t kSmemBytes = size_t(kInRing + kOutRing + 2 * kBitmapSmemWords) * sizeof(uint32_t);
+constexpr uint32_t kHashSlots = 2 * kS;      // open-addressing table: load factor <= 1/2
+// Shared memory after the rings: two bitmaps (bitmap probe) or one hash table (hash probe).
+__host__ __device__ constexpr size_t smem_bytes(int inner) {
+    return size_t(kInRing + kOutRing + (inner == 2 ? kHashSlots : 2 * kBitmapSmemWords)) * sizeof(uint32_t);
+}
 static_assert((kOutRing & (kOutRing - 1)) == 0, "output ring is indexed modulo its size");
 static_assert(kS <= kOutRing, "one tile's matches must fit the output ring");
 constexpr uint32_t kEndTile = 0xffffffffu;
@@ -264,7 +268,7 @@ __device__ __forceinline__ uint64_t look_back(uint64_t* status, uint64_t t, uint
 // owns as a bit mask over a contiguous run of one staged set: the matched
 // values are src[start + x] for every set bit x, in ascending order, and the
 // runs of consecutive threads are consecutive.
-enum Inner { kMergePath = 0, kBitmapProbe = 1 };
+enum Inner { kMergePath = 0, kBitmapProbe = 1, kHashProbe = 2 };
 
 struct ThreadMatches {
     const uint32_t* src;
@@ -368,6 +372,59 @@ __device__ __forceinline__ ThreadMatches bitmap_inner(const uint32_t* sA, int na
     return {Y, j0, mask};
 }
 
+// Hash probe (the reference's hi, src/hi.cu:295-479, restricted to one tile):
+// the smaller set part is inserted into an open-addressing table in shared
+// memory (multiplicative hash, linear probing, load factor <= 1/2), the other
+// part probes it.  0xffffffff marks an empty slot; the value 0xffffffff itself
+// can only be the last element of a part and is carried by a flag instead.
+// The table is cleared at the start of every hash tile, once every consumer
+// thread is past the previous tile's probes (the element-output path's
+// per-tile scan barrier orders that already; count-only needs one more).
+constexpr uint32_t kHashEmpty = 0xffffffffu;
+__device__ __forceinline__ uint32_t hash_slot(uint32_t v) { return (v * 0x9e3779b1u) >> (32 - 13); }
+static_assert(kHashSlots == (1u << 13), "hash_slot yields 13 bits");
+
+__device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, const uint32_t* sB, int nb, int tid,
+                                                    uint32_t* table, uint32_t* s_has_max, bool need_barrier) {
+    if (need_barrier) named_barrier(kConsumerBar, kConsumers);
+    uint4* t4 = reinterpret_cast<uint4*>(table);
+    for (uint32_t w = tid; w < kHashSlots / 4; w += kConsumers)
+        t4[w] = make_uint4(kHashEmpty, kHashEmpty, kHashEmpty, kHashEmpty);
+    if (tid == 0) *s_has_max = 0u;
+    named_barrier(kConsumerBar, kConsumers);
+    const bool buildA = na <= nb;
+    const uint32_t* X = buildA ? sA : sB;
+    const uint32_t* Y = buildA ? sB : sA;
+    const int nx = buildA ? na : nb, ny = buildA ? nb : na;
+    for (int e = tid; e < nx; e += kConsumers) {
+        const uint32_t v = X[e];
+        if (v == kHashEmpty) {
+            *s_has_max = 1u;
+            continue;
+        }
+        uint32_t h = hash_slot(v);
+        while (atomicCAS(table + h, kHashEmpty, v) != kHashEmpty) h = (h + 1) & (kHashSlots - 1);
+    }
+    named_barrier(kConsumerBar, kConsumers);
+    const uint32_t has_max = *s_has_max;
+    const int r = ((ny + kConsumers - 1) / kConsumers) | 1;
+    const int j0 = min(tid * r, ny), j1 = min(j0 + r, ny);
+    uint32_t mask = 0;
+    for (int e = j0; e < j1; ++e) {
+        const uint32_t v = Y[e];
+        bool hit;
+        if (v == kHashEmpty) {
+            hit = has_max != 0;
+        } else {
+            uint32_t h = hash_slot(v), t;
+            while ((t = table[h]) != v && t != kHashEmpty) h = (h + 1) & (kHashSlots - 1);
+            hit = t == v;
+        }
+        mask |= (hit ? 1u : 0u) << (e - j0);
+    }
+    return {Y, j0, mask};
+}
+
 template <bool kOut, int kInner>
 __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     const uint32_t* __restrict__ A, uint64_t nA, const uint32_t* __restrict__ B, uint64_t nB,
@@ -385,6 +442,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     __shared__ InDesc in_desc[kSlots];
     __shared__ uint64_t s_in_end[kSlots];  // producer-private: ring end of the tile in each slot
     __shared__ uint32_t s_warp[2][kConsumerWarps];  // by tile parity: a warp may run one tile ahead
+    __shared__ uint32_t s_has_max;                  // hash probe: the table's part holds 0xffffffff
 
     uint32_t* err = reinterpret_cast<uint32_t*>(ws);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -585,7 +643,9 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
         ThreadMatches tm;
         bool buildA = true;
         uint32_t span = 0;
-        if (kInner == kBitmapProbe && bitmap_fits(sA, d.na, sB, d.nb, buildA, span)) {
+        if (kInner == kHashProbe && d.na > 0 && d.nb > 0 && min(d.na, d.nb) < static_cast<int>(kHashSlots)) {
+            tm = hash_inner(sA, d.na, sB, d.nb, tid, bitmaps, &s_has_max, !kOut);
+        } else if (kInner == kBitmapProbe && bitmap_fits(sA, d.na, sB, d.nb, buildA, span)) {
             const uint32_t buf = nbm & 1u;
             tm = bitmap_inner(sA, d.na, sB, d.nb, buildA, span, tid, bitmaps + buf * kBitmapSmemWords,
                               buf ? stale1 : stale0);
@@ -704,10 +764,10 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
 
     const uint64_t nGroups = (L.nTiles + kGroup - 1) / kGroup;
     auto launch = [&](auto kernel, uint32_t* out) -> si_status {
-        SI_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kSmemBytes)));
+        const size_t smem = smem_bytes(inner);
+        SI_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         int per_sm = 0;
-        SI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, kSmemBytes));
+        SI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem));
         if (per_sm < 1) return SI_ERR_UNSUPPORTED;
         const unsigned grid =
             static_cast<unsigned>(std::min<uint64_t>(nGroups, static_cast<uint64_t>(sm_count()) * per_sm));
@@ -717,12 +777,14 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
                         (void*)&nTiles, (void*)&w, (void*)&status, (void*)&out, (void*)&cap, (void*)&d_count};
         PhaseTimer timer("sisi_tile", stream);
         SI_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(grid), dim3(kBlock), args,
-                                                kSmemBytes, stream));
+                                                smem, stream));
         return SI_OK;
     };
     si_status st;
     if (inner == kBitmapProbe) {
         st = d_out ? launch(ip_tile_kernel<true, kBitmapProbe>, d_out) : launch(ip_tile_kernel<false, kBitmapProbe>, nullptr);
+    } else if (inner == kHashProbe) {
+        st = d_out ? launch(ip_tile_kernel<true, kHashProbe>, d_out) : launch(ip_tile_kernel<false, kHashProbe>, nullptr);
     } else {
         st = d_out ? launch(ip_tile_kernel<true, kMergePath>, d_out) : launch(ip_tile_kernel<false, kMergePath>, nullptr);
     }

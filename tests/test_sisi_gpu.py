@@ -9,7 +9,7 @@ from set_intersection_b200 import dataset as fmt
 
 pytestmark = pytest.mark.gpu
 
-TECHS = ["ip", "bitmap"]
+TECHS = ["ip", "bitmap", "hi", "obs", "auto"]
 
 
 def dev(x):
@@ -132,6 +132,26 @@ def test_plain_config_seeds_1_2(cuda, tech):
     from set_intersection_b200 import generate
     a, b = generate.sisi_plain()
     check(a, b, tech)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_skewed_config(cuda, tech):
+    """|A| = 2^16, |B| = 2^26 from [0, 2^30), 20 % of A planted into B."""
+    from set_intersection_b200 import generate
+    a, b = generate.sisi_skewed()
+    check(a, b, tech)
+    check(b, a, tech)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_hash_collisions_and_strides(cuda, tech):
+    """Values that share low bits or hash buckets: strided sets whose tiles are
+    dense arithmetic progressions."""
+    for stride in (1 << 13, 1 << 16, 4097, 3 << 20):
+        a = (np.arange(0, 60000, dtype=np.uint64) * stride % (1 << 32)).astype(np.uint32)
+        a = np.unique(a)
+        b = np.unique(np.concatenate([a[::3], a[1::5] + 1])).astype(np.uint32)
+        check(a, b, tech)
 
 
 @pytest.mark.parametrize("tech", TECHS)
