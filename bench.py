@@ -56,6 +56,14 @@ WORKLOADS = {
                         n=None, universe=1 << 30, seeds=(5,)),
     "misi_dense": dict(desc="MISI all pairs: 16384 sets over values [0,65536), Bernoulli(0.05) membership, seed 6",
                        k=16384, n_values=65536, p=0.05, seeds=(6,)),
+    "misi_powerlaw": dict(desc="MISI all pairs: 8192 sets, sizes ~ n^-1.1 on [16,65536], distinct values of "
+                               "[1,2^20] with Zipf(0.8) popularity, seed 7",
+                          kind="powerlaw", k=8192, n_min=16, n_max=65536, size_exp=1.1, universe=1 << 20,
+                          value_exp=0.8, seeds=(7,)),
+    "misi_powerlaw_small": dict(desc="MISI all pairs: the first 2048 sets of the power-law collection "
+                                     "(profiling size)",
+                                kind="powerlaw", k=2048, n_min=16, n_max=65536, size_exp=1.1, universe=1 << 20,
+                                value_exp=0.8, seeds=(7,)),
     "misi_dense_small": dict(desc="MISI all pairs: 4096 sets over values [0,65536), Bernoulli(0.05), seed 6 "
                                   "(incidence 256 MiB > L2; profiling size)",
                              k=4096, n_values=65536, p=0.05, seeds=(6,)),
@@ -381,69 +389,92 @@ def run_ours(args, rank: int, world: int):
 
 
 # ------------------------------------------------------- MISI, dense form --
-def dense_collection(name: str):
-    from set_intersection_b200 import generate
+def is_powerlaw(name: str) -> bool:
+    return WORKLOADS[name].get("kind") == "powerlaw"
+
+
+def misi_universe(name: str) -> int:
+    """Largest value of the workload's collection (the dataset header's universe)."""
     w = WORKLOADS[name]
-    return generate.bernoulli(w["seeds"][0], w["k"], w["n_values"], w["p"])
+    return w["universe"] if is_powerlaw(name) else w["n_values"] - 1
+
+
+def dense_collection(name: str):
+    return dense_sample(name, WORKLOADS[name]["k"])
 
 
 def dense_sample(name: str, k_sample: int):
-    """The first k_sample sets of the workload (same density and universe)."""
+    """The first k_sample sets of the workload (every set is drawn from its own
+    stream, so these are exactly the workload's first sets)."""
     from set_intersection_b200 import generate
     w = WORKLOADS[name]
+    if is_powerlaw(name):
+        return generate.powerlaw(w["seeds"][0], k_sample, w["n_min"], w["n_max"], w["size_exp"], w["universe"],
+                                 w["value_exp"])
     return generate.bernoulli(w["seeds"][0], k_sample, w["n_values"], w["p"])
 
 
-def dense_reference_ms(el, off, n_values: int, tmpdir: str, threads: int) -> float:
-    """One run of the reference's boost_bitset executable (all pairs, OpenMP)
-    on a dataset file; its own HostTimer figure for the intersection phase."""
+# CPU reference per all-pairs workload: executable, its HostTimer interval,
+# the oracle technique of the same algorithm, the sample size in sets
+CPU_REF = {
+    "dense": ("boost_bitset", "Boost bitset intersection", "bitset", 1024, "src/boost_bitset.cpp:60-84"),
+    "powerlaw": ("stdintersection", "std::set intersection", "std", 640, "src/std_set_intersection.cpp:58-76"),
+}
+
+
+def dense_reference_ms(el, off, universe: int, tmpdir: str, threads: int, exe: str, interval: str) -> float:
+    """One run of a reference CPU executable (all pairs, OpenMP) on a dataset
+    file; its own HostTimer figure for the intersection phase."""
     import oracle
     from set_intersection_b200 import dataset as fmt
-    path = os.path.join(tmpdir, "dense.bin")
+    path = os.path.join(tmpdir, "misi.bin")
     if not os.path.exists(path):
         sizes = np.diff(off).astype(np.uint32)
-        fmt.write_dataset(path, fmt.Dataset(len(sizes), n_values - 1, sizes, el))
-    r = oracle.run_ref("boost_bitset", path, threads=threads)
-    return r["host_ms"]["Boost bitset intersection"]
+        fmt.write_dataset(path, fmt.Dataset(len(sizes), universe, sizes, el))
+    r = oracle.run_ref(exe, path, threads=threads)
+    return r["host_ms"][interval]
 
 
-def dense_port_ms(el, off, n_values: int, threads: int) -> float:
+def dense_port_ms(el, off, universe: int, threads: int, tech: str) -> float:
     import oracle
     k = off.size - 1
     t0 = time.perf_counter()
-    oracle.all_pairs(el, off, k, n_values - 1, "bitset", threads=threads)
+    oracle.all_pairs(el, off, k, universe, tech, threads=threads)
     return (time.perf_counter() - t0) * 1e3
 
 
-def dense_cpu_measure(name: str, k_sample: int, steps: int, warmup: int):
+def dense_cpu_measure(name: str, k_sample: int | None, steps: int, warmup: int):
     import oracle
+    exe, interval, port_tech, k_default, cite = CPU_REF["powerlaw" if is_powerlaw(name) else "dense"]
+    k_sample = k_sample or k_default
     el, off = dense_sample(name, k_sample)
-    n_values = WORKLOADS[name]["n_values"]
+    universe = misi_universe(name)
     threads = os.cpu_count() or 1
-    kind = "reference" if oracle.ref_binary("boost_bitset") else "port"
+    kind = "reference" if oracle.ref_binary(exe) else "port"
     times = []
     with tempfile.TemporaryDirectory() as td:
         for i in range(warmup + steps):
-            ms = (dense_reference_ms(el, off, n_values, td, threads) if kind == "reference"
-                  else dense_port_ms(el, off, n_values, threads))
+            ms = (dense_reference_ms(el, off, universe, td, threads, exe, interval) if kind == "reference"
+                  else dense_port_ms(el, off, universe, threads, port_tech))
             if i >= warmup:
                 times.append(ms)
     ms = statistics.median(times)
     pairs = k_sample * (k_sample - 1) // 2
-    desc = (f"first {k_sample} sets of the workload ({pairs} pairs), boost_bitset --threads {threads} "
-            f"(src/boost_bitset.cpp:60-84), median of {steps} runs timed by its HostTimer")
+    desc = (f"first {k_sample} sets of the workload ({pairs} pairs), {exe} --threads {threads} "
+            f"({cite}), median of {steps} runs timed by its HostTimer")
     return kind, threads, pairs / (ms * 1e-3), desc, ms
 
 
 def run_reference_dense(args, rank: int):
     if rank != 0:
         return
-    kind, threads, value, desc, ms = dense_cpu_measure(args.workload, 1024, args.steps, args.warmup)
+    kind, threads, value, desc, ms = dense_cpu_measure(args.workload, None, args.steps, args.warmup)
     line = {
         "impl": "reference", "metric": "MISI pairs/s", "value": value, "unit": "pairs/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "technique": "boost_bitset"},
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
+                   "technique": CPU_REF["powerlaw" if is_powerlaw(args.workload) else "dense"][0]},
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind, "sample": desc},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -463,11 +494,15 @@ def run_ours_dense(args, rank: int, world: int):
         import torch.distributed as dist_mod
         dist = dist_mod
         dist.init_process_group("nccl", device_id=dev)
-    tech = args.technique if args.technique in ("mm", "bitmap_naive") else "mm"
+    powerlaw = is_powerlaw(args.workload)
+    if powerlaw:
+        tech = args.technique if args.technique in ("ip", "obs", "hi", "bitmap", "auto") else "bitmap"
+    else:
+        tech = args.technique if args.technique in ("mm", "bitmap_naive") else "mm"
     dtype = args.dtype
     w = WORKLOADS[args.workload]
     el, off = dense_collection(args.workload)
-    k, universe = off.size - 1, w["n_values"] - 1
+    k, universe = off.size - 1, misi_universe(args.workload)
     pairs = k * (k - 1) // 2
     stream = torch.cuda.Stream(dev)
     col = api.Collection(torch.from_numpy(el.view(np.int32)).to(dev), torch.from_numpy(off).to(dev), universe)
@@ -475,7 +510,10 @@ def run_ours_dense(args, rank: int, world: int):
     counts = torch.empty(pairs, dtype=torch.int32, device=dev)
 
     def step(t=tech, d=dtype, out=counts):
-        api.misi_dense_into(col, out, t, d, ws, stream)
+        if t in ("mm", "bitmap_naive"):
+            api.misi_dense_into(col, out, t, d, ws, stream)
+        else:
+            api.misi_into(col, out, t, workspace=ws, stream=stream)
 
     # parity of the benchmarked call, once, before timing: against the plain
     # popcount kernel on every pair and the oracle on sampled pairs
@@ -485,7 +523,7 @@ def run_ours_dense(args, rank: int, world: int):
     if rank == 0 and not args.no_parity:
         import oracle
         plain = torch.empty_like(counts)
-        api.misi_dense_into(col, plain, "bitmap_naive", "int8", ws, stream)
+        step(t="ip" if powerlaw else "bitmap_naive", d="int8", out=plain)
         ws.check(stream)
         same = bool(torch.equal(plain, counts))
         rng = np.random.default_rng(1)
@@ -495,7 +533,8 @@ def run_ours_dense(args, rank: int, world: int):
         idx = pairs - (k - a) * (k - a - 1) // 2 + b - a - 1
         got = counts.cpu().numpy().view(np.uint32)[idx]
         parity = same and bool(np.array_equal(got, want))
-        log(f"parity: all pairs vs plain kernel {same}, 20000 sampled pairs vs oracle {np.array_equal(got, want)}")
+        log(f"parity: all pairs vs {'ip' if powerlaw else 'plain'} kernel {same}, "
+            f"20000 sampled pairs vs oracle {np.array_equal(got, want)}")
         del plain
 
     for _ in range(args.warmup):
@@ -505,7 +544,7 @@ def run_ours_dense(args, rank: int, world: int):
         dist.barrier()
     torch.cuda.synchronize()
 
-    gemm_phase = b"mm_gemm" if tech == "mm" else b"naive_popcount"
+    gemm_phase = b"misi_probe" if powerlaw else b"mm_gemm" if tech == "mm" else b"naive_popcount"
     lib.si_timer_reset()
     lib.si_timer_enable(1)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -550,7 +589,10 @@ def run_ours_dense(args, rank: int, world: int):
         h_off = torch.from_numpy(off).pin_memory()
         h_counts = torch.empty(pairs, dtype=torch.int32).pin_memory()
         ctx = api.HostCollection(dev)
-        api.misi_dense_host(h_el, h_off, universe, tech, dtype, h_counts, ctx, stream)
+        if powerlaw:
+            api.misi_host(h_el, h_off, universe, tech, h_counts, ctx, stream)
+        else:
+            api.misi_dense_host(h_el, h_off, universe, tech, dtype, h_counts, ctx, stream)
         e_steps = max(1, min(args.steps, args.e2e_steps))
         if dist:
             dist.barrier()
@@ -558,7 +600,10 @@ def run_ours_dense(args, rank: int, world: int):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(e_steps):
-            api.misi_dense_host(h_el, h_off, universe, tech, dtype, h_counts, ctx, stream)
+            if powerlaw:
+                api.misi_host(h_el, h_off, universe, tech, h_counts, ctx, stream)
+            else:
+                api.misi_dense_host(h_el, h_off, universe, tech, dtype, h_counts, ctx, stream)
         e1.record(stream)
         e1.synchronize()
         e_ms = e0.elapsed_time(e1)
@@ -589,29 +634,47 @@ def run_ours_dense(args, rank: int, world: int):
                 "avg_launch_ms": avg_ms, "launches": int(k_n.value),
                 "peak_source": ("2 x measured dense bf16 (8-bit operands run at twice the 16-bit rate)"
                                 if "bf16_tflops" in peaks else "2 x fallback bf16")}
+    elif powerlaw:
+        # algorithmic bytes: every pair reads its smaller set once (4 B per
+        # probe), each set is read once more as the staged side, and every
+        # pair writes its count
+        sizes = np.sort(np.diff(off))[::-1]
+        suffix = np.cumsum(sizes[::-1])[::-1]
+        probes = int(suffix[1:].sum())
+        alg_bytes = 4 * probes + 4 * int(el.size) + 4 * pairs
+        peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
+        achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": f"misi_probe_kernel<{tech}>", "alg_bytes_per_launch": alg_bytes,
+                "probes_per_launch": probes, "avg_launch_ms": avg_ms, "launches": int(k_n.value),
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "note": "probe reads of the smaller sets are mostly served by L2; HBM is the conservative peak"}
     else:
         roof = {"bound": "alu", "achieved": None, "peak": None, "unit": None, "frac": None, "traffic": None,
                 "kernel": "popcount_gemm_kernel", "avg_launch_ms": avg_ms, "launches": int(k_n.value)}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        kind, threads, cval, desc, _ = dense_cpu_measure(args.workload, 1024, steps=3, warmup=1)
+        kind, threads, cval, desc, _ = dense_cpu_measure(args.workload, None, steps=3, warmup=1)
         cpu = {"value": cval, "unit": "pairs/s", "cores": threads, "kind": kind, "sample": desc}
 
     line = {
         "metric": "MISI pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8" if dtype == "int8" else "e4m3",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32" if powerlaw else "u8" if dtype == "int8" else "e4m3",
         "data": "synthetic",
-        "config": {"workload": args.workload, "desc": w["desc"], "technique": tech, "operand": dtype,
-                   "k": k, "values": w["n_values"], "pairs": pairs, "elements": int(el.size),
-                   "l2": f"incidence operand {w['k'] * w['n_values'] >> 20} MiB per step > 126 MB L2; no flush",
+        "config": {"workload": args.workload, "desc": w["desc"], "technique": tech,
+                   "operand": None if powerlaw else dtype,
+                   "k": k, "universe": universe, "pairs": pairs, "elements": int(el.size),
+                   "l2": ("collection and counts per step > 126 MB L2 at 8192 sets; no flush" if powerlaw else
+                          f"incidence operand {w['k'] * w['n_values'] >> 20} MiB per step > 126 MB L2; no flush"),
                    "parallelism": f"replicas{world}", "parity_vs_oracle": parity,
                    "plain_popcount_ms_per_step": plain_ms,
                    "speedup_vs_plain": (plain_ms / ms_step) if plain_ms else None},
         "roofline": roof,
         "e2e": e2e,
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": (4 if powerlaw else 2) * args.steps,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
     }
@@ -640,7 +703,7 @@ def main():
         p.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
-    dense = args.workload.startswith("misi_dense")
+    dense = args.workload.startswith("misi_")
     if args.impl == "reference":
         (run_reference_dense if dense else run_reference_arm)(args, rank)
     else:

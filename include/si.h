@@ -123,6 +123,33 @@ si_status si_workspace_diagnostic(const void* d_workspace, si_stream_t stream, u
  * to d_flag (device uint32).  No workspace. */
 si_status si_validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, si_stream_t stream);
 
+/* ------------------------------------------------------------------ MISI --
+ * All pairs between two ranges of sets of a collection (one tile pair of the
+ * reference's MISI loop, include/util.hpp:24-52).
+ *
+ * d_elements / d_offsets: the collection in CSR form on the device (set i is
+ * d_elements[d_offsets[i] .. d_offsets[i+1]), sets ascending and duplicate
+ * free, each below 2^32 elements).  A, B: set ranges [start, end).
+ *  - A == B (self-join tile): every pair a < b of the range;
+ *    counts[tri(stride, a - A.start, b - A.start)], tri = include/util.hpp:68-70.
+ *  - A != B (cross tile, disjoint ranges): every pair (a in A, b in B);
+ *    counts[(a - A.start) * stride + (b - B.start)] (include/util.hpp:72-74).
+ * stride is the reference's numOfSets: the cardinality for the single-tile
+ * run (A = B = {0, k}), else the partition size.  Every count of the tile is
+ * written (zero for pairs with an empty set).
+ *
+ * Replaces the per-run kernels of src/ip.cu:141-177 (findDiagonals +
+ * intersectPath), src/obs.cu:275-438 (warpBasedOBS / blockBasedOBS),
+ * src/hi.cu:295-420 (warpBasedHI / blockBasedHI) and
+ * src/bitmap_dynamic.cu:240-319.  t: IP, OBS, HI, BITMAP or AUTO (= BITMAP).
+ * MM and BITMAP_NAIVE are served by si_misi_dense (single-tile run only).
+ */
+typedef struct si_set_range { uint32_t start, end; } si_set_range;
+size_t si_misi_workspace_size(si_set_range A, si_set_range B, si_technique t);
+si_status si_misi(const uint32_t* d_elements, const uint64_t* d_offsets, si_set_range A, si_set_range B,
+                  uint64_t stride, si_technique t, uint32_t* d_counts, void* d_workspace, size_t workspace_bytes,
+                  si_stream_t stream);
+
 /* --------------------------------------------------- MISI, dense form --
  * All pairs a < b of a collection of k sets over values 0..universe:
  * counts[tri(k, a, b)] = |S_a ∩ S_b|, tri = include/util.hpp:68-70 (the
@@ -151,7 +178,9 @@ si_status si_misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, u
  * DeviceTimer (include/device_timer.cuh:20-78), which wraps every phase of
  * every executable the same way.  Phase names: single pair "sisi_prepare",
  * "sisi_split", "sisi_tile"; dense all pairs "mm_incidence", "mm_gemm",
- * "naive_bitmaps", "naive_popcount".  si_timer_read synchronises on
+ * "naive_bitmaps", "naive_popcount"; all pairs of a tile "misi_plan",
+ * "misi_probe"; single pair by search "obs_sample", "obs_search", "obs_scan",
+ * "obs_compact".  si_timer_read synchronises on
  * the recorded events and returns the summed milliseconds and the number of
  * launches of one phase.
  */
@@ -175,6 +204,13 @@ si_status si_gen_uniform(uint64_t seed, uint64_t n, uint64_t lo, uint64_t hi, ui
  * same offsets to fill the sets (each ascending). */
 si_status si_gen_bernoulli(uint64_t seed, uint32_t k, uint32_t n_values, double p, uint64_t* offsets,
                            uint32_t* elements, int threads);
+
+/* si_gen_powerlaw: k sets with sizes from the power law P(n) ~ n^-size_exp on
+ * [n_min, n_max] and distinct values of [1, universe] drawn with Zipf
+ * popularity P(v) ~ v^-value_exp.  Same two-call protocol as
+ * si_gen_bernoulli.  n_max <= universe. */
+si_status si_gen_powerlaw(uint64_t seed, uint32_t k, uint32_t n_min, uint32_t n_max, double size_exp,
+                          uint32_t universe, double value_exp, uint64_t* offsets, uint32_t* elements, int threads);
 
 #ifdef __cplusplus
 }

@@ -58,6 +58,12 @@ _u64 = ctypes.c_uint64
 _sz = ctypes.c_size_t
 _int = ctypes.c_int
 
+
+class SetRange(ctypes.Structure):
+    """si_set_range: sets [start, end) of a collection."""
+    _fields_ = [("start", ctypes.c_uint32), ("end", ctypes.c_uint32)]
+
+
 _SIGNATURES = {
     "si_version": (ctypes.c_char_p, []),
     "si_status_string": (ctypes.c_char_p, [_int]),
@@ -70,6 +76,10 @@ _SIGNATURES = {
     "si_validate_sorted": (_int, [_vp, _u64, _vp, _vp]),
     "si_gen_uniform": (_int, [_u64, _u64, _u64, _u64, _vp, _int]),
     "si_gen_bernoulli": (_int, [_u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, _vp, _vp, _int]),
+    "si_gen_powerlaw": (_int, [_u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,
+                               ctypes.c_uint32, ctypes.c_double, _vp, _vp, _int]),
+    "si_misi_workspace_size": (_sz, [SetRange, SetRange, _int]),
+    "si_misi": (_int, [_vp, _vp, SetRange, SetRange, _u64, _int, _vp, _vp, _sz, _vp]),
     "si_misi_dense_workspace_size": (_sz, [ctypes.c_uint32, ctypes.c_uint32, _int]),
     "si_misi_dense": (_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _int, _int, _vp, _vp, _sz, _vp]),
     "si_timer_enable": (None, [_int]),

@@ -205,6 +205,68 @@ def misi_dense(col: Collection, tech="mm", dtype="int8", workspace: Workspace | 
     return counts[: n_pairs(col.k)]
 
 
+def _range(r, k):
+    from ._lib import SetRange
+    if r is None:
+        return SetRange(0, k)
+    return SetRange(int(r[0]), int(r[1]))
+
+
+def misi_count_size(a_range, b_range, stride: int) -> int:
+    """Counts written by one tile pair (triangular self-join or quadratic cross)."""
+    na = a_range[1] - a_range[0]
+    if tuple(a_range) == tuple(b_range):
+        if na < 2:
+            return 0
+        i, j = na - 2, na - 1
+        return stride * (stride - 1) // 2 - (stride - i) * (stride - i - 1) // 2 + j - i - 1 + 1
+    nb = b_range[1] - b_range[0]
+    return (na - 1) * stride + nb if na and nb else 0
+
+
+def misi_into(col: Collection, counts: torch.Tensor, tech="bitmap", a_range=None, b_range=None,
+              stride: int | None = None, workspace: Workspace | None = None, stream=None) -> None:
+    """Asynchronous all-pairs call over one tile pair of the collection
+    (default: the whole collection as one self-join tile, triangular order)."""
+    t = technique(tech)
+    a = _range(a_range, col.k)
+    b = _range(b_range if b_range is not None else a_range, col.k)
+    self_join = (a.start, a.end) == (b.start, b.end)
+    if stride is None:
+        stride = (a.end - a.start) if self_join else (b.end - b.start)
+    need = misi_count_size((a.start, a.end), (b.start, b.end), stride)
+    if counts.numel() < need or not counts.is_cuda:
+        raise ValueError(f"counts must be a CUDA tensor of >= {need} elements")
+    ws = workspace if workspace is not None else Workspace(col.elements.device)
+    buf = ws.get(lib.si_misi_workspace_size(a, b, int(t)))
+    st = lib.si_misi(_ptr(col.elements), _ptr(col.offsets), a, b, stride, int(t), _ptr(counts), _ptr(buf),
+                     buf.numel(), _stream(stream))
+    check(st, "si_misi")
+
+
+def misi(col: Collection, tech="bitmap", a_range=None, b_range=None, stride: int | None = None,
+         workspace: Workspace | None = None, stream=None, check_errors: bool = True) -> torch.Tensor:
+    """Counts of one tile pair (default: all pairs a < b, triangular order).
+    Techniques ip, obs, hi, bitmap, auto; mm and bitmap_naive go to the dense
+    path (whole collection only)."""
+    t = technique(tech)
+    if t in (Technique.MM, Technique.BITMAP_NAIVE):
+        if a_range is not None or b_range is not None:
+            raise ValueError("dense techniques count the whole collection only")
+        return misi_dense(col, tech, workspace=workspace, stream=stream, check_errors=check_errors)
+    ws = workspace or Workspace(col.elements.device)
+    a = (0, col.k) if a_range is None else tuple(a_range)
+    b = a if b_range is None else tuple(b_range)
+    if stride is None:
+        stride = (a[1] - a[0]) if a == b else (b[1] - b[0])
+    n = misi_count_size(a, b, stride)
+    counts = torch.empty(max(1, n), dtype=torch.int32, device=col.elements.device)
+    misi_into(col, counts, tech, a, b, stride, ws, stream)
+    if check_errors:
+        ws.check(stream)
+    return counts[:n]
+
+
 class HostCollection:
     """Device buffers and workspace reused by misi_dense_host across calls."""
 
@@ -235,14 +297,25 @@ def misi_dense_host(elements_host: torch.Tensor, offsets_host: torch.Tensor, uni
     ctx.counts = ctx._fit(ctx.counts, n_pairs(k), torch.int32)
     if counts_host is None:
         counts_host = torch.empty(max(1, n_pairs(k)), dtype=torch.int32).pin_memory()
+    dense = technique(tech) in (Technique.MM, Technique.BITMAP_NAIVE)
     with torch.cuda.stream(s):
         ctx.el[:n].copy_(elements_host.view(torch.int32), non_blocking=True)
         ctx.off[:k + 1].copy_(offsets_host, non_blocking=True)
         col = Collection(ctx.el[:n], ctx.off[:k + 1], universe)
-        misi_dense_into(col, ctx.counts, tech, dtype, ctx.ws, s)
+        if dense:
+            misi_dense_into(col, ctx.counts, tech, dtype, ctx.ws, s)
+        else:
+            misi_into(col, ctx.counts, tech, workspace=ctx.ws, stream=s)
         counts_host[:n_pairs(k)].copy_(ctx.counts[:n_pairs(k)], non_blocking=True)
     ctx.ws.check(s)
     return counts_host[:n_pairs(k)]
+
+
+def misi_host(elements_host: torch.Tensor, offsets_host: torch.Tensor, universe: int, tech="bitmap",
+              counts_host: torch.Tensor | None = None, ctx: HostCollection | None = None, stream=None):
+    """End-to-end all pairs of a HOST collection with any technique (dense
+    ones included): H2D, count every pair a < b, D2H of the counts."""
+    return misi_dense_host(elements_host, offsets_host, universe, tech, "int8", counts_host, ctx, stream)
 
 
 def validate_sorted(x: torch.Tensor, stream=None) -> bool:
@@ -256,8 +329,8 @@ def status_string(s: int) -> str:
     return lib.si_status_string(int(s)).decode()
 
 
-__all__ = ["Status", "Technique", "Workspace", "HostPair", "Collection", "HostCollection", "misi_dense", "misi_dense_into",
-           "misi_dense_host", "intersect", "intersect_host",
+__all__ = ["Status", "Technique", "Workspace", "HostPair", "Collection", "HostCollection", "misi", "misi_into", "misi_dense", "misi_dense_into",
+           "misi_dense_host", "misi_host", "intersect", "intersect_host",
            "sisi_into",
            "sisi_workspace_size",
            "technique", "validate_sorted", "status_string"]

@@ -169,6 +169,33 @@ si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
     }
 }
 
+size_t si_misi_workspace_size(si_set_range A, si_set_range B, si_technique t) {
+    if (t != SI_TECH_IP && t != SI_TECH_OBS && t != SI_TECH_HI && t != SI_TECH_BITMAP && t != SI_TECH_AUTO) return 0;
+    if (A.end < A.start || B.end < B.start) return 0;
+    return si::misi_workspace_size(A, B);
+}
+
+si_status si_misi(const uint32_t* d_elements, const uint64_t* d_offsets, si_set_range A, si_set_range B,
+                  uint64_t stride, si_technique t, uint32_t* d_counts, void* d_workspace, size_t workspace_bytes,
+                  si_stream_t stream) {
+    if (t == SI_TECH_MM || t == SI_TECH_BITMAP_NAIVE) return SI_ERR_UNSUPPORTED;  // si_misi_dense
+    if (t != SI_TECH_IP && t != SI_TECH_OBS && t != SI_TECH_HI && t != SI_TECH_BITMAP && t != SI_TECH_AUTO)
+        return SI_ERR_INVALID_ARGUMENT;
+    if (!d_offsets || !d_workspace || !d_counts) return SI_ERR_INVALID_ARGUMENT;
+    if (A.end < A.start || B.end < B.start) return SI_ERR_INVALID_ARGUMENT;
+    const bool self = A.start == B.start && A.end == B.end;
+    const uint64_t nA = A.end - A.start, nB = B.end - B.start;
+    if (!self && A.start < B.end && B.start < A.end) return SI_ERR_INVALID_ARGUMENT;  // overlapping ranges
+    if (stride < (self ? nA : nB)) return SI_ERR_INVALID_ARGUMENT;
+    if (nA + nB >= (1ull << 31)) return SI_ERR_UNSUPPORTED;
+    if (!si::aligned(d_elements, 4) || !si::aligned(d_offsets, 8) || !si::aligned(d_counts, 4) ||
+        !si::aligned(d_workspace, 256))
+        return SI_ERR_INVALID_ARGUMENT;
+    if (t == SI_TECH_AUTO) t = SI_TECH_BITMAP;
+    return si::misi_tile(d_elements, d_offsets, t, A, B, stride, d_counts, d_workspace, workspace_bytes,
+                         reinterpret_cast<cudaStream_t>(stream));
+}
+
 size_t si_misi_dense_workspace_size(uint32_t k, uint32_t universe, si_technique t) {
     if (t != SI_TECH_MM && t != SI_TECH_BITMAP_NAIVE) return 0;
     return si::dense_workspace_size(k, universe, t);

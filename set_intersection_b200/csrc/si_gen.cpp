@@ -14,7 +14,17 @@
 //
 // Bernoulli membership (a dense collection): value v is in set a iff
 // hash32(seed, a * 2^32 + v) < p * 2^32, independently for every (a, v).
+//
+// Power-law collection: set sizes from the continuous power law
+// P(n) ~ n^-size_exp on [n_min, n_max + 1), floored (inverse-CDF sampling);
+// each set then holds that many DISTINCT values of [1, universe] drawn with
+// Zipf popularity P(v) ~ v^-value_exp by rejection-inversion sampling
+// (Hormann and Derflinger, "Rejection-inversion to generate variates from
+// monotone discrete distributions", 1996), repeats rejected.  Every set has
+// its own random stream (splitmix64 of seed and set index), so the result
+// does not depend on the thread count.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <thread>
 #include <unordered_set>
@@ -136,8 +146,112 @@ void uniform_sparse(uint64_t seed, uint64_t n, uint64_t lo, uint64_t U, uint32_t
     std::sort(out, out + n);
 }
 
+// Uniform double in [0, 1) from a splitmix64 stream.
+struct Stream {
+    uint64_t state;
+    explicit Stream(uint64_t seed) : state(seed) {}
+    uint64_t next() {
+        state += 0x9e3779b97f4a7c15ull;
+        return mix64(state);
+    }
+    double uniform() { return static_cast<double>(next() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+// Zipf(s) over {1 .. N} by rejection-inversion.  H is an antiderivative of
+// h(x) = x^-s; a continuous variate is drawn by inverting H over
+// [H(1.5) - 1, H(N + 0.5)], rounded to the nearest integer k, and accepted if
+// it falls under h(k) (the test against shortcut_ accepts most draws without
+// evaluating H).
+class Zipf {
+  public:
+    Zipf(uint64_t n, double s) : n_(static_cast<double>(n)), s_(s) {
+        h_x1_ = H(1.5) - 1.0;
+        h_n_ = H(n_ + 0.5);
+        shortcut_ = 2.0 - Hinv(H(2.5) - h(2.0));
+    }
+    uint64_t operator()(Stream& rng) const {
+        for (;;) {
+            const double u = h_n_ + rng.uniform() * (h_x1_ - h_n_);
+            const double x = Hinv(u);
+            double k = std::floor(x + 0.5);
+            if (k < 1.0) k = 1.0;
+            if (k > n_) k = n_;
+            if (k - x <= shortcut_ || u >= H(k + 0.5) - h(k)) return static_cast<uint64_t>(k);
+        }
+    }
+
+  private:
+    double h(double x) const { return std::exp(-s_ * std::log(x)); }
+    // H(x) = (x^(1-s) - 1) / (1 - s), with its limit log(x) at s = 1
+    double H(double x) const {
+        const double lx = std::log(x);
+        return helper2((1.0 - s_) * lx) * lx;
+    }
+    double Hinv(double y) const {
+        double t = y * (1.0 - s_);
+        if (t < -1.0) t = -1.0;  // rounding guard: x >= 0
+        return std::exp(helper1(t) * y);
+    }
+    // helper1(t) = log(1 + t) / t, helper2(t) = (exp(t) - 1) / t, both -> 1 at t = 0
+    static double helper1(double t) { return std::fabs(t) > 1e-8 ? std::log1p(t) / t : 1.0 - t / 2.0; }
+    static double helper2(double t) { return std::fabs(t) > 1e-8 ? std::expm1(t) / t : 1.0 + t / 2.0; }
+    double n_, s_, h_x1_ = 0, h_n_ = 0, shortcut_ = 0;
+};
+
+uint64_t powerlaw_size(uint64_t seed, uint64_t a, uint32_t n_min, uint32_t n_max, double e) {
+    Stream rng(mix64(seed * 0x2545f4914f6cdd1dull + a));
+    const double u = rng.uniform();
+    const double lo = n_min, hi = static_cast<double>(n_max) + 1.0;
+    double x;
+    if (std::fabs(e - 1.0) < 1e-12) {
+        x = lo * std::exp(u * std::log(hi / lo));
+    } else {
+        const double q = 1.0 - e;
+        x = std::pow(std::pow(lo, q) + u * (std::pow(hi, q) - std::pow(lo, q)), 1.0 / q);
+    }
+    const uint64_t n = static_cast<uint64_t>(std::floor(x));
+    return std::min<uint64_t>(std::max<uint64_t>(n, n_min), n_max);
+}
+
 }  // namespace
 }  // namespace si
+
+extern "C" si_status si_gen_powerlaw(uint64_t seed, uint32_t k, uint32_t n_min, uint32_t n_max, double size_exp,
+                                     uint32_t universe, double value_exp, uint64_t* offsets, uint32_t* elements,
+                                     int threads) {
+    if (!offsets || n_min == 0 || n_min > n_max || n_max > universe || !(size_exp > 0.0) || !(value_exp >= 0.0))
+        return SI_ERR_INVALID_ARGUMENT;
+    const int T = si::resolve_threads(threads);
+    if (!elements) {
+        offsets[0] = 0;
+        si::parallel_chunks(k, T, [&](int, uint64_t b, uint64_t e) {
+            for (uint64_t a = b; a < e; ++a) offsets[a + 1] = si::powerlaw_size(seed, a, n_min, n_max, size_exp);
+        });
+        for (uint32_t a = 0; a < k; ++a) offsets[a + 1] += offsets[a];
+        return SI_OK;
+    }
+    const si::Zipf zipf(universe, value_exp);
+    si::parallel_chunks(k, T, [&](int, uint64_t b, uint64_t e) {
+        std::vector<uint64_t> seen((static_cast<uint64_t>(universe) >> 6) + 1);
+        for (uint64_t a = b; a < e; ++a) {
+            const uint64_t n = offsets[a + 1] - offsets[a];
+            si::Stream rng(si::mix64(seed * 0x9e3779b97f4a7c15ull + 0x51ed270b2da3ab9bull + a));
+            std::vector<uint32_t> vals;
+            vals.reserve(n);
+            while (vals.size() < n) {
+                const uint64_t v = zipf(rng);
+                uint64_t& w = seen[v >> 6];
+                if (w & (1ull << (v & 63))) continue;
+                w |= 1ull << (v & 63);
+                vals.push_back(static_cast<uint32_t>(v));
+            }
+            for (uint32_t v : vals) seen[v >> 6] &= ~(1ull << (v & 63));
+            std::sort(vals.begin(), vals.end());
+            std::copy(vals.begin(), vals.end(), elements + offsets[a]);
+        }
+    });
+    return SI_OK;
+}
 
 extern "C" si_status si_gen_bernoulli(uint64_t seed, uint32_t k, uint32_t n_values, double p, uint64_t* offsets,
                                       uint32_t* elements, int threads) {

@@ -60,6 +60,10 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
 // ---- all pairs of a dense collection (si_misi_dense.cu) ----
 // t: SI_TECH_MM (tensor cores; fp8 selects FP8-e4m3 operands instead of INT8)
 // or SI_TECH_BITMAP_NAIVE (plain AND-popcount on CUDA cores).
+size_t misi_workspace_size(si_set_range A, si_set_range B);
+si_status misi_tile(const uint32_t* d_elements, const uint64_t* d_offsets, si_technique t, si_set_range A,
+                    si_set_range B, uint64_t stride, uint32_t* d_counts, void* ws, size_t ws_bytes,
+                    cudaStream_t stream);
 size_t dense_workspace_size(uint32_t k, uint32_t universe, si_technique t);
 si_status misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint32_t universe,
                      si_technique t, int fp8, uint32_t* d_counts, void* ws, size_t ws_bytes, cudaStream_t stream);

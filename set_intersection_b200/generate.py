@@ -71,3 +71,26 @@ def misi_dense(seed: int = 6, k: int = 16384, n_values: int = 65536, p: float = 
     """The dense all-pairs collection: 16384 sets over 65536 values,
     Bernoulli(0.05) membership."""
     return bernoulli(seed, k, n_values, p)
+
+
+def powerlaw(seed: int, k: int, n_min: int, n_max: int, size_exp: float, universe: int, value_exp: float,
+             threads: int = 0):
+    """k sets, sizes ~ n^-size_exp on [n_min, n_max], distinct values of
+    [1, universe] with Zipf(value_exp) popularity.  Set a depends only on
+    (seed, a), so the first j sets of a collection are the collection of j
+    sets.  Returns (elements uint32, offsets int64[k + 1])."""
+    offsets = np.empty(k + 1, dtype=np.uint64)
+    args = (seed, k, n_min, n_max, size_exp, universe, value_exp)
+    st = lib.si_gen_powerlaw(*args, offsets.ctypes.data_as(ctypes.c_void_p), None, threads)
+    check(st, "si_gen_powerlaw")
+    elements = np.empty(int(offsets[-1]), dtype=np.uint32)
+    st = lib.si_gen_powerlaw(*args, offsets.ctypes.data_as(ctypes.c_void_p),
+                             elements.ctypes.data_as(ctypes.c_void_p), threads)
+    check(st, "si_gen_powerlaw")
+    return elements, offsets.astype(np.int64)
+
+
+def misi_powerlaw(seed: int = 7, k: int = 8192):
+    """The power-law all-pairs collection: 8192 sets, sizes ~ n^-1.1 on
+    [16, 65536], values of [1, 2^20] with Zipf(0.8) popularity."""
+    return powerlaw(seed, k, 16, 65536, 1.1, 1 << 20, 0.8)

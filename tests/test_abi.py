@@ -98,6 +98,50 @@ def test_bernoulli_generator_density_and_determinism():
     assert empty_el.size == 0 and np.all(empty_off == 0)
 
 
+def test_misi_invalid_arguments_rejected_on_host():
+    L = si.lib
+    R = _lib.SetRange
+    nul = ctypes.c_void_p(None)
+    fake = ctypes.c_void_p(0x1000)
+    bm = int(Technique.BITMAP)
+    ws = 1 << 30
+    # dense techniques belong to si_misi_dense
+    assert L.si_misi(fake, fake, R(0, 10), R(0, 10), 10, int(Technique.MM), fake, fake, ws, nul) == Status.UNSUPPORTED
+    assert L.si_misi(fake, fake, R(0, 10), R(0, 10), 10, 42, fake, fake, ws, nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi(fake, nul, R(0, 10), R(0, 10), 10, bm, fake, fake, ws, nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi(fake, fake, R(0, 10), R(0, 10), 10, bm, nul, fake, ws, nul) == Status.INVALID_ARGUMENT
+    # overlapping cross ranges, reversed range, stride below the tile
+    assert L.si_misi(fake, fake, R(0, 10), R(5, 15), 10, bm, fake, fake, ws, nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi(fake, fake, R(10, 5), R(10, 5), 10, bm, fake, fake, ws, nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi(fake, fake, R(0, 10), R(0, 10), 9, bm, fake, fake, ws, nul) == Status.INVALID_ARGUMENT
+    assert L.si_misi(fake, fake, R(0, 10), R(10, 30), 19, bm, fake, fake, ws, nul) == Status.INVALID_ARGUMENT
+    # workspace too small is detected before any launch
+    need = L.si_misi_workspace_size(R(0, 8192), R(0, 8192), bm)
+    assert need > 8192 * 8
+    assert L.si_misi(fake, fake, R(0, 8192), R(0, 8192), 8192, bm, fake, fake, need - 1,
+                     nul) == Status.WORKSPACE_TOO_SMALL
+    assert L.si_misi_workspace_size(R(0, 10), R(0, 10), int(Technique.MM)) == 0
+
+
+def test_powerlaw_generator_sizes_values_and_determinism():
+    from set_intersection_b200 import generate
+    el, off = generate.powerlaw(5, 400, 16, 4096, 1.1, 1 << 16, 0.8, threads=3)
+    el2, off2 = generate.powerlaw(5, 400, 16, 4096, 1.1, 1 << 16, 0.8, threads=7)
+    assert np.array_equal(el, el2) and np.array_equal(off, off2)
+    sizes = np.diff(off)
+    assert sizes.min() >= 16 and sizes.max() <= 4096 and off[-1] == el.size
+    # a power law with exponent 1.1 puts most sets near the lower end
+    assert np.median(sizes) < sizes.mean() < 4096 / 2
+    for a in range(400):
+        s = el[off[a]:off[a + 1]]
+        assert np.all(np.diff(s.astype(np.int64)) > 0) and s[0] >= 1 and s[-1] <= 1 << 16
+    # Zipf popularity: small values are far more common than large ones
+    assert np.count_nonzero(el <= 64) > 20 * np.count_nonzero((el > (1 << 16) - 64))
+    # set a depends only on (seed, a): a prefix of the collection is the smaller collection
+    el3, off3 = generate.powerlaw(5, 100, 16, 4096, 1.1, 1 << 16, 0.8)
+    assert np.array_equal(el3, el[:off[100]]) and np.array_equal(off3, off[:101])
+
+
 def test_workspace_size_grows_with_input():
     f = si.lib.si_sisi_workspace_size
     small = f(1000, 1000, int(Technique.IP))
