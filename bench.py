@@ -64,6 +64,12 @@ WORKLOADS = {
                                      "(profiling size)",
                                 kind="powerlaw", k=2048, n_min=16, n_max=65536, size_exp=1.1, universe=1 << 20,
                                 value_exp=0.8, seeds=(7,)),
+    "batch_pairs": dict(desc="Batched pairs: pool of 100000 sets, sizes log-uniform on [32,2^18], distinct values of "
+                             "[0,2^26); 1M pairs (i,j), i != j, uniform over the pool; counts only; seeds 8, 9",
+                        kind="batch", k=100000, npairs=1000000, seeds=(8,)),
+    "batch_pairs_small": dict(desc="Batched pairs: a tenth of the batched workload (10000 sets, 100000 pairs; "
+                                   "profiling size)",
+                              kind="batch", k=10000, npairs=100000, seeds=(8,)),
     "misi_dense_small": dict(desc="MISI all pairs: 4096 sets over values [0,65536), Bernoulli(0.05), seed 6 "
                                   "(incidence 256 MiB > L2; profiling size)",
                              k=4096, n_values=65536, p=0.05, seeds=(6,)),
@@ -683,6 +689,223 @@ def run_ours_dense(args, rank: int, world: int):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------ batched pairs --
+def batch_data(name: str):
+    from set_intersection_b200 import generate
+    w = WORKLOADS[name]
+    return generate.batch_pool(seed=w["seeds"][0], k=w["k"], npairs=w["npairs"])
+
+
+def batch_cpu_measure(el, off, pairs, n_sample: int, steps: int, warmup: int):
+    """The oracle's per-pair std::set_intersection count (the reference's
+    std_set_intersection loop body, src/std_set_intersection.cpp:58-76, run on
+    a pair list with OpenMP) on the first n_sample pairs: the reference has no
+    pair-list executable, so this is a port."""
+    import oracle
+    threads = os.cpu_count() or 1
+    sample = pairs[:n_sample]
+    k = off.size - 1
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        oracle.pairs(el, off, k, sample, threads=threads)
+        if i >= warmup:
+            times.append((time.perf_counter() - t0) * 1e3)
+    ms = statistics.median(times)
+    desc = (f"first {n_sample} pairs of the workload, std::set_intersection per pair, {threads} threads, "
+            f"median of {steps} runs")
+    return "port", threads, n_sample / (ms * 1e-3), desc, ms
+
+
+def run_reference_batch(args, rank: int):
+    if rank != 0:
+        return
+    el, off, pairs = batch_data(args.workload)
+    kind, threads, value, desc, ms = batch_cpu_measure(el, off, pairs, 20000, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": "batched pairs/s", "value": value, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
+                   "technique": "std::set_intersection per pair"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind, "sample": desc},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours_batch(args, rank: int, world: int):
+    import ctypes
+    import torch
+    from set_intersection_b200 import api
+    from set_intersection_b200._lib import lib
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        dist.init_process_group("nccl", device_id=dev)
+    w = WORKLOADS[args.workload]
+    el, off, pairs = batch_data(args.workload)
+    k, npairs = off.size - 1, len(pairs)
+    stream = torch.cuda.Stream(dev)
+    col = api.Collection(torch.from_numpy(el.view(np.int32)).to(dev), torch.from_numpy(off).to(dev), (1 << 26) - 1)
+    dpairs = torch.from_numpy(pairs.view(np.int32)).to(dev)
+    counts = torch.empty(npairs, dtype=torch.int32, device=dev)
+    ws = api.Workspace(dev)
+    tech = args.technique if args.technique in ("ip", "obs", "auto") else "auto"
+
+    t0 = time.perf_counter()
+    table = api.batch_tune(col, dpairs, workspace=ws, stream=stream) if tech == "auto" else None
+    tune_s = time.perf_counter() - t0
+    graph = api.BatchGraph(col, dpairs, counts, tech, table, workspace=api.Workspace(dev))
+
+    graph.launch(stream)
+    graph.check(stream)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        import oracle
+        idx = np.random.default_rng(3).choice(npairs, 20000, replace=False)
+        got = counts.cpu().numpy().view(np.uint32)
+        parity = bool(np.array_equal(got[idx], oracle.pairs(el, off, k, pairs[idx])))
+        log(f"parity: 20000 sampled pairs vs oracle {parity}")
+
+    for _ in range(args.warmup):
+        graph.launch(stream)
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    lib.si_timer_reset()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            graph.launch(stream)
+        stop.record(stream)
+        stop.synchronize()
+    ms_total = start.elapsed_time(stop)
+    graph.check(stream)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * npairs / (ms_step * 1e-3)
+
+    # the batch kernel alone (phase timer on a direct call, outside the graph)
+    lib.si_timer_enable(1)
+    for _ in range(3):
+        api.batch_count_into(col, dpairs, counts, tech, table, ws, stream)
+    stream.synchronize()
+    lib.si_timer_enable(0)
+    k_ms, k_n = ctypes.c_double(0), ctypes.c_uint64(0)
+    lib.si_timer_read(b"batch_count", ctypes.byref(k_ms), ctypes.byref(k_n))
+    lib.si_timer_reset()
+    kern_ms = k_ms.value / max(1, k_n.value)
+
+    # plain: one single-pair call per pair (3 launches each), on a sample
+    plain = None
+    if not args.no_plain:
+        n_plain = 2000
+        a_t = [col.elements[int(off[i]):int(off[i + 1])] for i in range(k)]
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        pws = api.Workspace(dev)
+        for i in range(50):
+            api.sisi_into(a_t[pairs[i, 0]], a_t[pairs[i, 1]], cnt, None, pws, "ip", stream)
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for i in range(n_plain):
+            api.sisi_into(a_t[pairs[i, 0]], a_t[pairs[i, 1]], cnt, None, pws, "ip", stream)
+        p1.record(stream)
+        p1.synchronize()
+        pms = p0.elapsed_time(p1)
+        plain = {"pairs_per_s": n_plain / (pms * 1e-3), "sample_pairs": n_plain,
+                 "desc": "si_sisi(ip) per pair on the first 2000 pairs, one call (3 launches) each"}
+
+    e2e = None
+    if not args.no_e2e:
+        h_pairs = torch.from_numpy(pairs.view(np.int32)).pin_memory()
+        h_counts = torch.empty(npairs, dtype=torch.int32).pin_memory()
+        e_steps = max(1, min(args.steps, args.e2e_steps))
+
+        def e2e_step():
+            with torch.cuda.stream(stream):
+                dpairs.copy_(h_pairs, non_blocking=True)
+                graph.launch(stream)
+                h_counts.copy_(counts, non_blocking=True)
+            stream.synchronize()
+
+        e2e_step()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e_steps):
+            e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        e_ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e_step = e_ms / e_steps
+        e2e = {"value": world * npairs / (e_step * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": int(8 * npairs),
+               "d2h_bytes_per_step": int(4 * npairs), "ms_per_step": e_step, "steps": e_steps,
+               "note": "pool resident in HBM (the indexed collection); per step the query pairs go H2D and "
+                       "the counts D2H through the graph"}
+    graph.close()
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    sizes = np.diff(off)
+    merge_elems = int(sizes[pairs[:, 0]].sum() + sizes[pairs[:, 1]].sum())
+    alg_bytes = 4 * merge_elems + 12 * npairs
+    peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "batch_kernel", "alg_bytes_per_launch": alg_bytes,
+            "avg_launch_ms": kern_ms, "launches": int(k_n.value),
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "note": "algorithmic bytes of a full merge of every pair (4 B per element of both sets, pairs and "
+                    "counts); search-technique pairs read less, so frac can exceed what a merge could reach"}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        kind, threads, cval, desc, _ = batch_cpu_measure(el, off, pairs, 20000, steps=3, warmup=1)
+        cpu = {"value": cval, "unit": "pairs/s", "cores": threads, "kind": kind, "sample": desc}
+    tb = np.frombuffer(table, np.uint8) if table is not None else None
+    line = {
+        "metric": "batched pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"], "technique": tech, "k": k, "pairs": npairs,
+                   "elements": int(el.size), "merge_elements": merge_elems,
+                   "l2": f"pool {el.size * 4 >> 20} MiB > 126 MB L2; no flush",
+                   "graph": "one CUDA graph per step: key kernel, radix sort of the queue, batch kernel",
+                   "autotune_s": tune_s if table is not None else None,
+                   "search_buckets": int(tb.sum()) if tb is not None else None,
+                   "parallelism": f"replicas{world}", "parity_vs_oracle": parity,
+                   "plain_per_pair": plain,
+                   "speedup_vs_plain": (value / world / plain["pairs_per_s"]) if plain else None},
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -696,18 +919,19 @@ def main():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-parity", action="store_true")
-    p.add_argument("--no-plain", action="store_true", help="dense: skip timing the plain popcount kernel")
+    p.add_argument("--no-plain", action="store_true",
+                   help="dense / batch: skip timing the plain kernel (popcount / one call per pair)")
     p.add_argument("--dtype", choices=["int8", "fp8"], default="int8", help="dense: tensor-core operand type")
     args = p.parse_args()
     if args.warmup < 3:
         p.error("--warmup must be >= 3")
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
-    dense = args.workload.startswith("misi_")
+    kind = "misi" if args.workload.startswith("misi_") else "batch" if args.workload.startswith("batch_") else "sisi"
     if args.impl == "reference":
-        (run_reference_dense if dense else run_reference_arm)(args, rank)
+        {"misi": run_reference_dense, "batch": run_reference_batch, "sisi": run_reference_arm}[kind](args, rank)
     else:
-        (run_ours_dense if dense else run_ours)(args, rank, world)
+        {"misi": run_ours_dense, "batch": run_ours_batch, "sisi": run_ours}[kind](args, rank, world)
 
 
 if __name__ == "__main__":

@@ -150,6 +150,44 @@ si_status si_misi(const uint32_t* d_elements, const uint64_t* d_offsets, si_set_
                   uint64_t stride, si_technique t, uint32_t* d_counts, void* d_workspace, size_t workspace_bytes,
                   si_stream_t stream);
 
+/* --------------------------------------------------------- batched pairs --
+ * Counts of a list of pairs of one collection, in one persistent launch.  No
+ * counterpart in the reference, which launches kernels per pair
+ * (src/ip.cu:141-177); this is the batched form of the single-pair count.
+ *
+ * d_pairs: device uint32[2 * npairs], pair p = (d_pairs[2p], d_pairs[2p+1]),
+ * set indices < k.  d_counts: device uint32[npairs], counts[p] = |S_a ∩ S_b|.
+ * t = SI_TECH_IP: every pair by streaming merge; SI_TECH_OBS: every pair by
+ * binary search of the smaller set in the larger; SI_TECH_AUTO: per bucket of
+ * (log2 smaller size, log2 size ratio) from `table` (host uint8[256],
+ * bucket = (min(15, log2 s) << 4) | min(15, log2(l / s)), 0 = merge,
+ * 1 = search), or, with table == NULL, search when l >= 16 s.
+ * npairs < 2^32.
+ */
+size_t si_batch_workspace_size(uint64_t npairs);
+si_status si_batch_count(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
+                         uint64_t npairs, si_technique t, const uint8_t* table, uint32_t* d_counts,
+                         void* d_workspace, size_t workspace_bytes, si_stream_t stream);
+
+/* The autotuner: times merge and search on up to `sample` pairs of every
+ * bucket that holds at least 32 pairs of this batch and writes the faster
+ * choice per bucket to table_out (host uint8[256]; other buckets keep the
+ * default).  Synchronises the stream; overwrites d_counts. */
+si_status si_batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
+                        uint64_t npairs, uint32_t sample, uint32_t* d_counts, void* d_workspace,
+                        size_t workspace_bytes, si_stream_t stream, uint8_t* table_out);
+
+/* The same batch captured once into a CUDA graph (all of si_batch_count's
+ * launches for these pointers and sizes), replayed by si_batch_graph_launch on
+ * any stream.  The buffers must stay valid while the graph exists. */
+typedef struct si_batch_graph si_batch_graph;
+si_status si_batch_graph_create(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k,
+                                const uint32_t* d_pairs, uint64_t npairs, si_technique t, const uint8_t* table,
+                                uint32_t* d_counts, void* d_workspace, size_t workspace_bytes,
+                                si_batch_graph** out);
+si_status si_batch_graph_launch(si_batch_graph* graph, si_stream_t stream);
+void si_batch_graph_destroy(si_batch_graph* graph);
+
 /* --------------------------------------------------- MISI, dense form --
  * All pairs a < b of a collection of k sets over values 0..universe:
  * counts[tri(k, a, b)] = |S_a ∩ S_b|, tri = include/util.hpp:68-70 (the
@@ -180,7 +218,7 @@ si_status si_misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, u
  * "sisi_split", "sisi_tile"; dense all pairs "mm_incidence", "mm_gemm",
  * "naive_bitmaps", "naive_popcount"; all pairs of a tile "misi_plan",
  * "misi_probe"; single pair by search "obs_sample", "obs_search", "obs_scan",
- * "obs_compact".  si_timer_read synchronises on
+ * "obs_compact"; batched pairs "batch_plan", "batch_count".  si_timer_read synchronises on
  * the recorded events and returns the summed milliseconds and the number of
  * launches of one phase.
  */
@@ -209,6 +247,11 @@ si_status si_gen_bernoulli(uint64_t seed, uint32_t k, uint32_t n_values, double 
  * [n_min, n_max] and distinct values of [1, universe] drawn with Zipf
  * popularity P(v) ~ v^-value_exp.  Same two-call protocol as
  * si_gen_bernoulli.  n_max <= universe. */
+/* si_gen_loguniform: k sets with sizes log-uniform on [n_min, n_max] and
+ * distinct values of [0, universe) drawn uniformly.  Same two-call protocol as
+ * si_gen_bernoulli.  n_max <= universe / 2. */
+si_status si_gen_loguniform(uint64_t seed, uint32_t k, uint32_t n_min, uint32_t n_max, uint32_t universe,
+                            uint64_t* offsets, uint32_t* elements, int threads);
 si_status si_gen_powerlaw(uint64_t seed, uint32_t k, uint32_t n_min, uint32_t n_max, double size_exp,
                           uint32_t universe, double value_exp, uint64_t* offsets, uint32_t* elements, int threads);
 

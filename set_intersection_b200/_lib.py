@@ -79,6 +79,15 @@ _SIGNATURES = {
     "si_gen_powerlaw": (_int, [_u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,
                                ctypes.c_uint32, ctypes.c_double, _vp, _vp, _int]),
     "si_misi_workspace_size": (_sz, [SetRange, SetRange, _int]),
+    "si_gen_loguniform": (_int, [_u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp,
+                                 _int]),
+    "si_batch_workspace_size": (_sz, [_u64]),
+    "si_batch_count": (_int, [_vp, _vp, ctypes.c_uint32, _vp, _u64, _int, _vp, _vp, _vp, _sz, _vp]),
+    "si_batch_tune": (_int, [_vp, _vp, ctypes.c_uint32, _vp, _u64, ctypes.c_uint32, _vp, _vp, _sz, _vp, _vp]),
+    "si_batch_graph_create": (_int, [_vp, _vp, ctypes.c_uint32, _vp, _u64, _int, _vp, _vp, _vp, _sz,
+                                     ctypes.POINTER(_vp)]),
+    "si_batch_graph_launch": (_int, [_vp, _vp]),
+    "si_batch_graph_destroy": (None, [_vp]),
     "si_misi": (_int, [_vp, _vp, SetRange, SetRange, _u64, _int, _vp, _vp, _sz, _vp]),
     "si_misi_dense_workspace_size": (_sz, [ctypes.c_uint32, ctypes.c_uint32, _int]),
     "si_misi_dense": (_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _int, _int, _vp, _vp, _sz, _vp]),

@@ -267,6 +267,90 @@ def misi(col: Collection, tech="bitmap", a_range=None, b_range=None, stride: int
     return counts[:n]
 
 
+def _pairs(pairs: torch.Tensor) -> int:
+    if not pairs.is_cuda or pairs.dtype not in (torch.int32, torch.uint32) or not pairs.is_contiguous() or \
+            pairs.dim() != 2 or pairs.shape[1] != 2:
+        raise ValueError("pairs must be a contiguous CUDA int32/uint32 tensor of shape [n, 2]")
+    return pairs.shape[0]
+
+
+def batch_count_into(col: Collection, pairs: torch.Tensor, counts: torch.Tensor, tech="auto",
+                     table: bytes | None = None, workspace: Workspace | None = None, stream=None) -> None:
+    """Asynchronous batched call: counts[p] <- |S_a ∩ S_b| for pair p = pairs[p]
+    (tech: "ip" = merge for all, "obs" = search for all, "auto" = per bucket
+    from `table`, the 256-byte output of batch_tune, or the default rule)."""
+    n = _pairs(pairs)
+    if counts.numel() < n or not counts.is_cuda:
+        raise ValueError("counts must be a CUDA tensor of len(pairs) elements")
+    ws = workspace if workspace is not None else Workspace(col.elements.device)
+    buf = ws.get(lib.si_batch_workspace_size(n))
+    tb = ctypes.create_string_buffer(bytes(table), 256) if table is not None else None
+    st = lib.si_batch_count(_ptr(col.elements), _ptr(col.offsets), col.k, _ptr(pairs), n, int(technique(tech)),
+                            tb, _ptr(counts), _ptr(buf), buf.numel(), _stream(stream))
+    check(st, "si_batch_count")
+
+
+def batch_count(col: Collection, pairs: torch.Tensor, tech="auto", table: bytes | None = None,
+                workspace: Workspace | None = None, stream=None, check_errors: bool = True) -> torch.Tensor:
+    ws = workspace or Workspace(col.elements.device)
+    counts = torch.empty(max(1, _pairs(pairs)), dtype=torch.int32, device=col.elements.device)
+    batch_count_into(col, pairs, counts, tech, table, ws, stream)
+    if check_errors:
+        ws.check(stream)
+    return counts[:pairs.shape[0]]
+
+
+def batch_tune(col: Collection, pairs: torch.Tensor, sample: int = 4096, workspace: Workspace | None = None,
+               stream=None) -> bytes:
+    """Times merge and search per (size, ratio) bucket of this batch; returns
+    the 256-byte technique table for batch_count(..., "auto", table)."""
+    n = _pairs(pairs)
+    ws = workspace or Workspace(col.elements.device)
+    buf = ws.get(lib.si_batch_workspace_size(n))
+    counts = torch.empty(max(1, n), dtype=torch.int32, device=col.elements.device)
+    out = ctypes.create_string_buffer(256)
+    st = lib.si_batch_tune(_ptr(col.elements), _ptr(col.offsets), col.k, _ptr(pairs), n, sample, _ptr(counts),
+                           _ptr(buf), buf.numel(), _stream(stream), out)
+    check(st, "si_batch_tune")
+    ws.check(stream)
+    return out.raw
+
+
+class BatchGraph:
+    """A batched call captured once into a CUDA graph and replayed by launch()."""
+
+    def __init__(self, col: Collection, pairs: torch.Tensor, counts: torch.Tensor, tech="auto",
+                 table: bytes | None = None, workspace: Workspace | None = None):
+        n = _pairs(pairs)
+        self.ws = workspace or Workspace(col.elements.device)
+        self.buf = self.ws.get(lib.si_batch_workspace_size(n))
+        self._keep = (col, pairs, counts)  # the graph holds their addresses
+        tb = ctypes.create_string_buffer(bytes(table), 256) if table is not None else None
+        h = ctypes.c_void_p()
+        st = lib.si_batch_graph_create(_ptr(col.elements), _ptr(col.offsets), col.k, _ptr(pairs), n,
+                                       int(technique(tech)), tb, _ptr(counts), _ptr(self.buf), self.buf.numel(),
+                                       ctypes.byref(h))
+        check(st, "si_batch_graph_create")
+        self.handle = h
+
+    def launch(self, stream=None) -> None:
+        check(lib.si_batch_graph_launch(self.handle, _stream(stream)), "si_batch_graph_launch")
+
+    def check(self, stream=None) -> None:
+        self.ws.check(stream)
+
+    def close(self) -> None:
+        if self.handle:
+            lib.si_batch_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class HostCollection:
     """Device buffers and workspace reused by misi_dense_host across calls."""
 
@@ -330,7 +414,8 @@ def status_string(s: int) -> str:
 
 
 __all__ = ["Status", "Technique", "Workspace", "HostPair", "Collection", "HostCollection", "misi", "misi_into", "misi_dense", "misi_dense_into",
-           "misi_dense_host", "misi_host", "intersect", "intersect_host",
+           "misi_dense_host", "misi_host", "batch_count", "batch_count_into",
+           "batch_tune", "BatchGraph", "intersect", "intersect_host",
            "sisi_into",
            "sisi_workspace_size",
            "technique", "validate_sorted", "status_string"]

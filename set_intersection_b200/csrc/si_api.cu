@@ -196,6 +196,90 @@ si_status si_misi(const uint32_t* d_elements, const uint64_t* d_offsets, si_set_
                          reinterpret_cast<cudaStream_t>(stream));
 }
 
+size_t si_batch_workspace_size(uint64_t npairs) { return si::batch_workspace_size(npairs); }
+
+static si_status batch_args(const uint32_t* d_elements, const uint64_t* d_offsets, const uint32_t* d_pairs,
+                            uint64_t npairs, si_technique t, uint32_t* d_counts, void* d_workspace) {
+    if (t != SI_TECH_IP && t != SI_TECH_OBS && t != SI_TECH_AUTO) return SI_ERR_INVALID_ARGUMENT;
+    if (!d_offsets || !d_workspace || (npairs && (!d_pairs || !d_counts))) return SI_ERR_INVALID_ARGUMENT;
+    if (npairs >= (1ull << 32)) return SI_ERR_UNSUPPORTED;
+    if (!si::aligned(d_elements, 4) || !si::aligned(d_offsets, 8) || !si::aligned(d_pairs, 4) ||
+        !si::aligned(d_counts, 4) || !si::aligned(d_workspace, 256))
+        return SI_ERR_INVALID_ARGUMENT;
+    return SI_OK;
+}
+
+si_status si_batch_count(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
+                         uint64_t npairs, si_technique t, const uint8_t* table, uint32_t* d_counts,
+                         void* d_workspace, size_t workspace_bytes, si_stream_t stream) {
+    const si_status st = batch_args(d_elements, d_offsets, d_pairs, npairs, t, d_counts, d_workspace);
+    if (st != SI_OK) return st;
+    return si::batch_count(d_elements, d_offsets, k, d_pairs, npairs, t, table, d_counts, d_workspace,
+                           workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+si_status si_batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
+                        uint64_t npairs, uint32_t sample, uint32_t* d_counts, void* d_workspace,
+                        size_t workspace_bytes, si_stream_t stream, uint8_t* table_out) {
+    if (!table_out || sample == 0) return SI_ERR_INVALID_ARGUMENT;
+    const si_status st = batch_args(d_elements, d_offsets, d_pairs, npairs, SI_TECH_AUTO, d_counts, d_workspace);
+    if (st != SI_OK) return st;
+    return si::batch_tune(d_elements, d_offsets, k, d_pairs, npairs, sample, d_counts, d_workspace,
+                          workspace_bytes, reinterpret_cast<cudaStream_t>(stream), table_out);
+}
+
+struct si_batch_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+si_status si_batch_graph_create(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k,
+                                const uint32_t* d_pairs, uint64_t npairs, si_technique t, const uint8_t* table,
+                                uint32_t* d_counts, void* d_workspace, size_t workspace_bytes,
+                                si_batch_graph** out) {
+    if (!out) return SI_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    si_status st = batch_args(d_elements, d_offsets, d_pairs, npairs, t, d_counts, d_workspace);
+    if (st != SI_OK) return st;
+    if (workspace_bytes < si::batch_workspace_size(npairs)) return SI_ERR_WORKSPACE_TOO_SMALL;
+    cudaStream_t cs = nullptr;
+    SI_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    auto* g = new si_batch_graph;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        st = si::batch_count(d_elements, d_offsets, k, d_pairs, npairs, t, table, d_counts, d_workspace,
+                             workspace_bytes, cs);
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &g->graph);
+        if (st == SI_OK && e2 != cudaSuccess) st = si::cuda_fail(e2, "cudaStreamEndCapture");
+        if (st == SI_OK) {
+            e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+            if (e != cudaSuccess) st = si::cuda_fail(e, "cudaGraphInstantiate");
+        }
+    } else {
+        st = si::cuda_fail(e, "cudaStreamBeginCapture");
+    }
+    cudaStreamDestroy(cs);
+    if (st != SI_OK) {
+        si_batch_graph_destroy(g);
+        return st;
+    }
+    *out = g;
+    return SI_OK;
+}
+
+si_status si_batch_graph_launch(si_batch_graph* graph, si_stream_t stream) {
+    if (!graph || !graph->exec) return SI_ERR_INVALID_ARGUMENT;
+    SI_CUDA_TRY(cudaGraphLaunch(graph->exec, reinterpret_cast<cudaStream_t>(stream)));
+    return SI_OK;
+}
+
+void si_batch_graph_destroy(si_batch_graph* graph) {
+    if (!graph) return;
+    if (graph->exec) cudaGraphExecDestroy(graph->exec);
+    if (graph->graph) cudaGraphDestroy(graph->graph);
+    delete graph;
+}
+
 size_t si_misi_dense_workspace_size(uint32_t k, uint32_t universe, si_technique t) {
     if (t != SI_TECH_MM && t != SI_TECH_BITMAP_NAIVE) return 0;
     return si::dense_workspace_size(k, universe, t);

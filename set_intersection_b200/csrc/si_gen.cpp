@@ -15,6 +15,9 @@
 // Bernoulli membership (a dense collection): value v is in set a iff
 // hash32(seed, a * 2^32 + v) < p * 2^32, independently for every (a, v).
 //
+// Log-uniform pool: sizes log-uniform on [n_min, n_max]; each set n distinct
+// uniform values of [0, universe).
+//
 // Power-law collection: set sizes from the continuous power law
 // P(n) ~ n^-size_exp on [n_min, n_max + 1), floored (inverse-CDF sampling);
 // each set then holds that many DISTINCT values of [1, universe] drawn with
@@ -215,6 +218,45 @@ uint64_t powerlaw_size(uint64_t seed, uint64_t a, uint32_t n_min, uint32_t n_max
 
 }  // namespace
 }  // namespace si
+
+extern "C" si_status si_gen_loguniform(uint64_t seed, uint32_t k, uint32_t n_min, uint32_t n_max, uint32_t universe,
+                                       uint64_t* offsets, uint32_t* elements, int threads) {
+    if (!offsets || n_min == 0 || n_min > n_max || static_cast<uint64_t>(n_max) * 2 > universe)
+        return SI_ERR_INVALID_ARGUMENT;
+    const int T = si::resolve_threads(threads);
+    if (!elements) {
+        offsets[0] = 0;
+        const double l0 = std::log(static_cast<double>(n_min)), l1 = std::log(static_cast<double>(n_max) + 1.0);
+        si::parallel_chunks(k, T, [&](int, uint64_t b, uint64_t e) {
+            for (uint64_t a = b; a < e; ++a) {
+                si::Stream rng(si::mix64(seed * 0x2545f4914f6cdd1dull + 0x3c6ef372fe94f82bull + a));
+                const uint64_t n = static_cast<uint64_t>(std::floor(std::exp(l0 + rng.uniform() * (l1 - l0))));
+                offsets[a + 1] = std::min<uint64_t>(std::max<uint64_t>(n, n_min), n_max);
+            }
+        });
+        for (uint32_t a = 0; a < k; ++a) offsets[a + 1] += offsets[a];
+        return SI_OK;
+    }
+    // n distinct values of [0, universe): n draws, sort, unique, and more draws
+    // for the few repeats until n are held
+    si::parallel_chunks(k, T, [&](int, uint64_t b, uint64_t e) {
+        std::vector<uint32_t> v;
+        for (uint64_t a = b; a < e; ++a) {
+            const uint64_t n = offsets[a + 1] - offsets[a];
+            si::Stream rng(si::mix64(seed * 0x9e3779b97f4a7c15ull + 0x7f4a7c159e3779b9ull + a));
+            v.clear();
+            while (v.size() < n) {
+                const size_t need = n - v.size();
+                for (size_t i = 0; i < need; ++i)
+                    v.push_back(static_cast<uint32_t>((static_cast<unsigned __int128>(rng.next()) * universe) >> 64));
+                std::sort(v.begin(), v.end());
+                v.erase(std::unique(v.begin(), v.end()), v.end());
+            }
+            std::copy(v.begin(), v.end(), elements + offsets[a]);
+        }
+    });
+    return SI_OK;
+}
 
 extern "C" si_status si_gen_powerlaw(uint64_t seed, uint32_t k, uint32_t n_min, uint32_t n_max, double size_exp,
                                      uint32_t universe, double value_exp, uint64_t* offsets, uint32_t* elements,

@@ -64,6 +64,13 @@ size_t misi_workspace_size(si_set_range A, si_set_range B);
 si_status misi_tile(const uint32_t* d_elements, const uint64_t* d_offsets, si_technique t, si_set_range A,
                     si_set_range B, uint64_t stride, uint32_t* d_counts, void* ws, size_t ws_bytes,
                     cudaStream_t stream);
+size_t batch_workspace_size(uint64_t npairs);
+si_status batch_count(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
+                      uint64_t npairs, si_technique t, const uint8_t* table, uint32_t* d_counts, void* ws,
+                      size_t ws_bytes, cudaStream_t stream);
+si_status batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
+                     uint64_t npairs, uint32_t sample, uint32_t* d_counts, void* ws, size_t ws_bytes,
+                     cudaStream_t stream, uint8_t* table_out);
 size_t dense_workspace_size(uint32_t k, uint32_t universe, si_technique t);
 si_status misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint32_t universe,
                      si_technique t, int fp8, uint32_t* d_counts, void* ws, size_t ws_bytes, cudaStream_t stream);

@@ -94,3 +94,32 @@ def misi_powerlaw(seed: int = 7, k: int = 8192):
     """The power-law all-pairs collection: 8192 sets, sizes ~ n^-1.1 on
     [16, 65536], values of [1, 2^20] with Zipf(0.8) popularity."""
     return powerlaw(seed, k, 16, 65536, 1.1, 1 << 20, 0.8)
+
+
+def loguniform(seed: int, k: int, n_min: int, n_max: int, universe: int, threads: int = 0):
+    """k sets, sizes log-uniform on [n_min, n_max], distinct uniform values of
+    [0, universe).  Returns (elements uint32, offsets int64[k + 1])."""
+    offsets = np.empty(k + 1, dtype=np.uint64)
+    st = lib.si_gen_loguniform(seed, k, n_min, n_max, universe, offsets.ctypes.data_as(ctypes.c_void_p), None,
+                               threads)
+    check(st, "si_gen_loguniform")
+    elements = np.empty(int(offsets[-1]), dtype=np.uint32)
+    st = lib.si_gen_loguniform(seed, k, n_min, n_max, universe, offsets.ctypes.data_as(ctypes.c_void_p),
+                               elements.ctypes.data_as(ctypes.c_void_p), threads)
+    check(st, "si_gen_loguniform")
+    return elements, offsets.astype(np.int64)
+
+
+def random_pairs(seed: int, k: int, npairs: int) -> np.ndarray:
+    """npairs pairs (i, j), i != j, drawn uniformly from [0, k): uint32[npairs, 2]."""
+    rng = np.random.default_rng(seed)
+    i = rng.integers(0, k, npairs, dtype=np.int64)
+    j = (i + rng.integers(1, k, npairs, dtype=np.int64)) % k
+    return np.stack([i, j], 1).astype(np.uint32)
+
+
+def batch_pool(seed: int = 8, k: int = 100000, npairs: int = 1000000):
+    """The batched-pairs workload: a pool of 100000 sets, sizes log-uniform on
+    [32, 2^18], values of [0, 2^26); 1M pairs drawn uniformly from the pool."""
+    el, off = loguniform(seed, k, 32, 1 << 18, 1 << 26)
+    return el, off, random_pairs(seed + 1, k, npairs)
