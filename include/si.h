@@ -75,7 +75,7 @@ const char* si_last_error_string(void);
  * std::set_intersection orders it.
  *
  * Techniques: IP merges, HI hashes and BITMAP bit-tests the two sets tile by
- * tile (value-pivot tiles of <= 4096 elements per set, both sets streamed
+ * tile (value-pivot tiles of <= 6144 elements per set, both sets streamed
  * once); OBS searches every element of the smaller set in the larger one
  * (cached top levels in shared memory); AUTO takes OBS when one set is more
  * than 64 times larger than the other, else BITMAP.

@@ -8,7 +8,7 @@
 //
 //  * Grid level: instead of one 32-thread warp probe per diagonal per pair,
 //    tiles are cut at VALUE pivots.  Every S-th element of A and of B is a
-//    pivot (S = 4096); a pivot's exact position in the other set is found with
+//    pivot (S = 6144); a pivot's exact position in the other set is found with
 //    one bounded binary search inside an S-element window that the sample
 //    merge identifies.  Consecutive pivots bound a tile to <= S elements of
 //    each set, and because a tile boundary is a value, an equal pair is never
@@ -30,7 +30,7 @@
 namespace si {
 namespace {
 
-constexpr uint32_t kS = 4096;                     // pivot (sample) stride
+constexpr uint32_t kS = 6144;                     // pivot (sample) stride
 constexpr int kPartials = 256;
 
 constexpr uint64_t kFlagAgg = 1ull << 62;
@@ -185,9 +185,9 @@ constexpr int kSlots = 8;
 constexpr int kOutQ = 16;                    // output descriptors in flight
 constexpr int kGroup = 4;                    // consecutive tiles per scheduling unit (one look-back each)
 constexpr uint32_t kInRing = 14336;          // u32: 56 KiB
-constexpr uint32_t kOutRing = 4096;          // u32: 16 KiB, a power of two
+constexpr uint32_t kOutRing = 8192;          // u32: 32 KiB, a power of two
 constexpr uint32_t kBitmapSmemWords = 2048;  // u32 per bitmap buffer (8 KiB); two buffers
-constexpr uint32_t kHashSlots = 2 * kS;      // open-addressing table: load factor <= 1/2
+constexpr uint32_t kHashSlots = 8192;        // open-addressing table: load factor <= 3/4
 // Shared memory after the rings: two bitmaps (bitmap probe) or one hash table (hash probe).
 __host__ __device__ constexpr size_t smem_bytes(int inner) {
     return size_t(kInRing + kOutRing + (inner == 2 ? kHashSlots : 2 * kBitmapSmemWords)) * sizeof(uint32_t);
@@ -198,7 +198,7 @@ constexpr uint32_t kEndTile = 0xffffffffu;
 constexpr uint32_t kConsumerBar = 1;  // named barrier id of the consumer warps
 
 static_assert(2 * (kS + 8) + 16 <= kInRing, "a tile's aligned superset must fit the input ring");
-static_assert((((2 * kS + kConsumers - 1) / kConsumers) | 1) <= 31, "per-thread match mask is 32 bits");
+static_assert((((2 * kS + kConsumers - 1) / kConsumers) | 1) <= 63, "per-thread match mask is 64 bits");
 static_assert(kGroup + 1 <= 32, "a group's split entries are held one per lane");
 
 struct InDesc {
@@ -273,7 +273,7 @@ enum Inner { kMergePath = 0, kBitmapProbe = 1, kHashProbe = 2 };
 struct ThreadMatches {
     const uint32_t* src;
     int start;
-    uint32_t mask;
+    uint64_t mask;
 };
 
 // Merge path (the reference's intersect-path, include/helpers.cuh:24-61): the
@@ -296,21 +296,23 @@ __device__ __forceinline__ ThreadMatches merge_inner(const uint32_t* sA, int na,
         len = c ? len - half - 1 : half;
     }
     const int i0 = lo;
-    uint32_t mask = 0;  // bit x: A element i0 + x is in B
+    uint64_t mask = 0;  // bit x: A element i0 + x is in B
     if (fast) {
         // sA[na] / sB[nb] are the successor elements of the ranges, both at or
         // above the next pivot and so above every value of the tile: they stop
-        // each side without bounds checks.  One shared load per step.
-        const uint32_t* pa = sA + i0;
-        const uint32_t* pb = sB + (d0 - i0);
-        uint32_t a = *pa, b = *pb, bit = 1u;
-        for (int s = d0; s < d1; ++s) {
+        // each side without bounds checks.  One shared load per step, through
+        // 32-bit shared-window byte addresses.
+        uint32_t pa = smem_addr(sA + i0), pb = smem_addr(sB + (d0 - i0));
+        uint32_t a = lds_u32(pa), b = lds_u32(pb), ka = 0;
+        const int steps = d1 - d0;
+#pragma unroll 4
+        for (int s = 0; s < steps; ++s) {
             const bool takeA = a <= b;
-            mask |= (a == b) ? bit : 0u;
-            bit = takeA ? bit << 1 : bit;
-            pa += takeA ? 1 : 0;
-            pb += takeA ? 0 : 1;
-            const uint32_t v = *(takeA ? pa : pb);
+            mask |= static_cast<uint64_t>(a == b) << ka;
+            ka += takeA ? 1u : 0u;
+            pa += takeA ? 4u : 0u;
+            pb += takeA ? 0u : 4u;
+            const uint32_t v = lds_u32(takeA ? pa : pb);
             a = takeA ? v : a;
             b = takeA ? b : v;
         }
@@ -320,7 +322,7 @@ __device__ __forceinline__ ThreadMatches merge_inner(const uint32_t* sA, int na,
             const bool aOk = i < na, bOk = j < nb;
             const uint32_t a = aOk ? sA[i] : 0u, b = bOk ? sB[j] : 0u;
             const bool takeA = aOk && (!bOk || a <= b);
-            if (takeA && bOk && a == b) mask |= 1u << (i - i0);
+            if (takeA && bOk && a == b) mask |= 1ull << (i - i0);
             if (takeA) ++i; else ++j;
         }
     }
@@ -362,19 +364,19 @@ __device__ __forceinline__ ThreadMatches bitmap_inner(const uint32_t* sA, int na
     named_barrier(kConsumerBar, kConsumers);
     const int r = ((ny + kConsumers - 1) / kConsumers) | 1;  // <= 15: one part holds <= kS values
     const int j0 = min(tid * r, ny), j1 = min(j0 + r, ny);
-    uint32_t mask = 0;
+    uint64_t mask = 0;
 #pragma unroll 4
     for (int e = j0; e < j1; ++e) {
         const uint32_t v = Y[e] - base;
         const uint32_t w = v <= span ? bm[v >> 5] : 0u;
-        mask |= ((w >> (v & 31)) & 1u) << (e - j0);
+        mask |= static_cast<uint64_t>((w >> (v & 31)) & 1u) << (e - j0);
     }
     return {Y, j0, mask};
 }
 
 // Hash probe (the reference's hi, src/hi.cu:295-479, restricted to one tile):
 // the smaller set part is inserted into an open-addressing table in shared
-// memory (multiplicative hash, linear probing, load factor <= 1/2), the other
+// memory (multiplicative hash, linear probing, load factor <= 3/4), the other
 // part probes it.  0xffffffff marks an empty slot; the value 0xffffffff itself
 // can only be the last element of a part and is carried by a flag instead.
 // The table is cleared at the start of every hash tile, once every consumer
@@ -409,7 +411,7 @@ __device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, 
     const uint32_t has_max = *s_has_max;
     const int r = ((ny + kConsumers - 1) / kConsumers) | 1;
     const int j0 = min(tid * r, ny), j1 = min(j0 + r, ny);
-    uint32_t mask = 0;
+    uint64_t mask = 0;
     for (int e = j0; e < j1; ++e) {
         const uint32_t v = Y[e];
         bool hit;
@@ -420,7 +422,7 @@ __device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, 
             while ((t = table[h]) != v && t != kHashEmpty) h = (h + 1) & (kHashSlots - 1);
             hit = t == v;
         }
-        mask |= (hit ? 1u : 0u) << (e - j0);
+        mask |= (hit ? 1ull : 0ull) << (e - j0);
     }
     return {Y, j0, mask};
 }
@@ -654,7 +656,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
         } else {
             tm = merge_inner(sA, d.na, sB, d.nb, d.fast != 0, tid);
         }
-        const uint32_t cnt = static_cast<uint32_t>(__popc(tm.mask));
+        const uint32_t cnt = static_cast<uint32_t>(__popcll(tm.mask));
 
         if constexpr (!kOut) {
             my_count += cnt;
@@ -693,10 +695,10 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
                 }
             }
             __syncwarp();
-            uint32_t m = tm.mask;
+            uint64_t m = tm.mask;
             uint64_t pos = ohead + incl - cnt + wsum;
             while (m) {
-                const int x = __ffs(m) - 1;
+                const int x = __ffsll(m) - 1;
                 m &= m - 1;
                 out_ring[pos++ & (kOutRing - 1)] = tm.src[tm.start + x];
             }
