@@ -203,6 +203,9 @@ void si_batch_graph_destroy(si_batch_graph* graph);
  *     comparison.  Replaces src/bitmap_naive.cu:433-441 (generateBitmaps +
  *     intersectPerPair).
  * d_counts: device uint32[k*(k-1)/2].
+ * Range: MM needs universe < 2^24 (every count exact in f32), BITMAP_NAIVE a
+ * universe whose bitmap fits 200 KiB (< 6.5M values); outside it the call
+ * returns SI_ERR_UNSUPPORTED and si_misi_dense_workspace_size returns 0.
  */
 typedef enum si_dense_dtype { SI_DENSE_INT8 = 0, SI_DENSE_FP8_E4M3 = 1 } si_dense_dtype;
 size_t si_misi_dense_workspace_size(uint32_t k, uint32_t universe, si_technique t);

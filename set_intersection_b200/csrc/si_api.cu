@@ -282,6 +282,7 @@ void si_batch_graph_destroy(si_batch_graph* graph) {
 
 size_t si_misi_dense_workspace_size(uint32_t k, uint32_t universe, si_technique t) {
     if (t != SI_TECH_MM && t != SI_TECH_BITMAP_NAIVE) return 0;
+    if (!si::dense_supported(universe, t)) return 0;
     return si::dense_workspace_size(k, universe, t);
 }
 
@@ -294,7 +295,7 @@ si_status si_misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, u
     if (!si::aligned(d_elements, 4) || !si::aligned(d_offsets, 8) || !si::aligned(d_counts, 4) ||
         !si::aligned(d_workspace, 256))
         return SI_ERR_INVALID_ARGUMENT;
-    if (universe >= (1u << 24)) return SI_ERR_UNSUPPORTED;  // counts must stay exact in f32
+    if (!si::dense_supported(universe, t)) return SI_ERR_UNSUPPORTED;
     return si::misi_dense(d_elements, d_offsets, k, universe, t, dtype == SI_DENSE_FP8_E4M3, d_counts,
                           d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
 }

@@ -71,6 +71,12 @@ si_status batch_count(const uint32_t* d_elements, const uint64_t* d_offsets, uin
 si_status batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
                      uint64_t npairs, uint32_t sample, uint32_t* d_counts, void* ws, size_t ws_bytes,
                      cudaStream_t stream, uint8_t* table_out);
+// The dense path's range: MM needs every count exact in f32 (universe < 2^24);
+// BITMAP_NAIVE builds one set's bitmap in shared memory (<= 200 KiB).
+inline bool dense_supported(uint32_t universe, si_technique t) {
+    if (t == SI_TECH_MM) return universe < (1u << 24);
+    return (static_cast<uint64_t>(universe) + 32) / 32 * 4 <= 200 * 1024;
+}
 size_t dense_workspace_size(uint32_t k, uint32_t universe, si_technique t);
 si_status misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint32_t universe,
                      si_technique t, int fp8, uint32_t* d_counts, void* ws, size_t ws_bytes, cudaStream_t stream);
