@@ -184,13 +184,19 @@ constexpr int kCtasPerSm = 2;
 constexpr int kSlots = 8;
 constexpr int kOutQ = 16;                    // output descriptors in flight
 constexpr int kGroup = 4;                    // consecutive tiles per scheduling unit (one look-back each)
-constexpr uint32_t kInRing = 14336;          // u32: 56 KiB
+constexpr uint32_t kInRing = 14336;          // u32: 56 KiB (the merge path adds the bitmap area: 72 KiB)
 constexpr uint32_t kOutRing = 8192;          // u32: 32 KiB, a power of two
 constexpr uint32_t kBitmapSmemWords = 2048;  // u32 per bitmap buffer (8 KiB); two buffers
-constexpr uint32_t kHashSlots = 8192;        // open-addressing table: load factor <= 3/4
+constexpr uint32_t kHashSlots = 4096;        // open-addressing table (16 KiB): load factor <= 1/2
 // Shared memory after the rings: two bitmaps (bitmap probe) or one hash table (hash probe).
+// Input ring of an inner loop: the merge path needs no bitmaps, so its ring
+// takes their space (about three average tiles instead of two).
+__host__ __device__ constexpr uint32_t in_ring_words(int inner) {
+    return inner == 0 ? kInRing + 2 * kBitmapSmemWords : kInRing;
+}
 __host__ __device__ constexpr size_t smem_bytes(int inner) {
-    return size_t(kInRing + kOutRing + (inner == 2 ? kHashSlots : 2 * kBitmapSmemWords)) * sizeof(uint32_t);
+    return size_t(in_ring_words(inner) + kOutRing + (inner == 2 ? kHashSlots : inner == 1 ? 2 * kBitmapSmemWords : 0)) *
+           sizeof(uint32_t);
 }
 static_assert((kOutRing & (kOutRing - 1)) == 0, "output ring is indexed modulo its size");
 static_assert(kS <= kOutRing, "one tile's matches must fit the output ring");
@@ -376,15 +382,17 @@ __device__ __forceinline__ ThreadMatches bitmap_inner(const uint32_t* sA, int na
 
 // Hash probe (the reference's hi, src/hi.cu:295-479, restricted to one tile):
 // the smaller set part is inserted into an open-addressing table in shared
-// memory (multiplicative hash, linear probing, load factor <= 3/4), the other
-// part probes it.  0xffffffff marks an empty slot; the value 0xffffffff itself
+// memory (multiplicative hash, linear probing, load factor <= 1/2), the other
+// part probes it.  A tile whose smaller part exceeds 2048 elements (half the
+// 16 KiB table) takes the merge path, which keeps two CTAs per SM.
+// 0xffffffff marks an empty slot; the value 0xffffffff itself
 // can only be the last element of a part and is carried by a flag instead.
 // The table is cleared at the start of every hash tile, once every consumer
 // thread is past the previous tile's probes (the element-output path's
 // per-tile scan barrier orders that already; count-only needs one more).
 constexpr uint32_t kHashEmpty = 0xffffffffu;
-__device__ __forceinline__ uint32_t hash_slot(uint32_t v) { return (v * 0x9e3779b1u) >> (32 - 13); }
-static_assert(kHashSlots == (1u << 13), "hash_slot yields 13 bits");
+__device__ __forceinline__ uint32_t hash_slot(uint32_t v) { return (v * 0x9e3779b1u) >> (32 - 12); }
+static_assert(kHashSlots == (1u << 12), "hash_slot yields 12 bits");
 
 __device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, const uint32_t* sB, int nb, int tid,
                                                     uint32_t* table, uint32_t* s_has_max, bool need_barrier) {
@@ -435,8 +443,9 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     uint64_t* __restrict__ d_count) {
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* in_ring = smem;
-    uint32_t* out_ring = smem + kInRing;
-    uint32_t* bitmaps = smem + kInRing + kOutRing;  // 2 x kBitmapSmemWords
+    constexpr uint32_t kRing = in_ring_words(kInner);
+    uint32_t* out_ring = smem + kRing;
+    uint32_t* bitmaps = smem + kRing + kOutRing;  // 2 x kBitmapSmemWords (bitmap) or the hash table
     __shared__ __align__(8) uint64_t full[kSlots], empty[kSlots], ofull[kOutQ], oempty[kOutQ];
     __shared__ __align__(8) uint64_t s_released_out;  // output ring: virtual offset written out so far
     __shared__ uint32_t s_otile[kOutQ], s_ocount[kOutQ];
@@ -554,10 +563,10 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
                         // A tile never wraps: if it does not fit before the ring's end it
                         // starts the next lap.  It may be placed once it overlaps no live
                         // tile: either every staged tile is released, or the live span
-                        // [released, head) ends at least kInRing before the tile's end.
-                        const uint64_t phys = head % kInRing;
-                        if (phys + need > kInRing) head += kInRing - phys;
-                        while (alive && k_rel < k && head + need - released > kInRing) alive = wait_release();
+                        // [released, head) ends at least kRing before the tile's end.
+                        const uint64_t phys = head % kRing;
+                        if (phys + need > kRing) head += kRing - phys;
+                        while (alive && k_rel < k && head + need - released > kRing) alive = wait_release();
                     }
                     if (!alive) {
                         if (t < nTiles) record_error(err, SI_ERR_TIMEOUT, 3, static_cast<uint32_t>(t));
@@ -566,7 +575,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
                             mbar_arrive(&full[slot]);
                         }
                     } else {
-                        const uint32_t base = static_cast<uint32_t>(head % kInRing);
+                        const uint32_t base = static_cast<uint32_t>(head % kRing);
                         head += need;
                         s_in_end[slot] = head;
                         InDesc& d = in_desc[slot];
@@ -645,7 +654,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
         ThreadMatches tm;
         bool buildA = true;
         uint32_t span = 0;
-        if (kInner == kHashProbe && d.na > 0 && d.nb > 0 && min(d.na, d.nb) < static_cast<int>(kHashSlots)) {
+        if (kInner == kHashProbe && d.na > 0 && d.nb > 0 && min(d.na, d.nb) <= static_cast<int>(kHashSlots / 2)) {
             tm = hash_inner(sA, d.na, sB, d.nb, tid, bitmaps, &s_has_max, !kOut);
         } else if (kInner == kBitmapProbe && bitmap_fits(sA, d.na, sB, d.nb, buildA, span)) {
             const uint32_t buf = nbm & 1u;
