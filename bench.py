@@ -2,7 +2,15 @@
 """Benchmark of the set-intersection hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sisi_large|sisi_plain|sisi_skewed] [--technique ip]
+                    [--workload W] [--technique T]
+
+Workloads: sisi_large (default), sisi_mid, sisi_plain, sisi_skewed (single
+pair, Gelem/s); misi_dense, misi_dense_small (all pairs on tensor cores or the
+plain popcount kernel, pairs/s); misi_powerlaw, misi_powerlaw_small (all pairs,
+ip/obs/hi/bitmap, pairs/s); batch_pairs, batch_pairs_small (1M pairs of a
+100000-set pool in one CUDA graph, pairs/s).  A default run (SISI, one GPU)
+also runs each other configuration briefly in a subprocess and adds a summary
+of each line under "other_workloads" (--no-extras skips them).
 
 One "step" is one pass of the single-pair (SISI) hot path over one pair of
 sets: the workload by default is |A| = |B| = 2^28 sorted unique uint32 drawn
@@ -389,6 +397,8 @@ def run_ours(args, rank: int, world: int):
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
     }
+    if world == 1 and not args.no_extras:
+        line["other_workloads"] = other_workloads(args)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -906,6 +916,41 @@ def run_ours_batch(args, rank: int, world: int):
         dist.destroy_process_group()
 
 
+# Short runs of the other configurations, for the record of a default run.
+EXTRAS = [
+    ("misi_dense", ["--technique", "mm", "--dtype", "int8"]),
+    ("misi_dense", ["--technique", "mm", "--dtype", "fp8", "--no-plain"]),
+    ("misi_powerlaw", ["--technique", "bitmap"]),
+    ("batch_pairs", ["--technique", "auto"]),
+    ("sisi_skewed", ["--technique", "auto"]),
+]
+
+
+def other_workloads(args) -> list:
+    out = []
+    for wl, extra in EXTRAS:
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", wl, "--steps", "5", "--warmup", "3",
+               "--no-e2e", "--no-cpu-baseline", "--no-extras", *extra]
+        t0 = time.time()
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            d = json.loads(r.stdout.strip().splitlines()[-1])
+        except Exception as e:  # recorded, not fatal: the headline line stands on its own
+            out.append({"workload": wl, "args": extra, "error": str(e)[:200]})
+            continue
+        roof = d.get("roofline") or {}
+        cfg = d.get("config") or {}
+        keep = {k: cfg[k] for k in ("technique", "operand", "parity_vs_oracle", "speedup_vs_plain",
+                                     "plain_popcount_ms_per_step", "plain_per_pair") if k in cfg}
+        out.append({"workload": wl, "metric": d["metric"], "value": d["value"], "unit": d["unit"],
+                    "ms_per_step": d["ms_per_step"], "steps": d["steps"],
+                    "roofline": {k: roof.get(k) for k in ("bound", "achieved", "peak", "unit", "frac", "kernel",
+                                                           "avg_launch_ms")},
+                    "clocks": d.get("clocks"), **keep, "wall_s": round(time.time() - t0, 1)})
+        log(f"{wl} {' '.join(extra)}: {d['value']:.4g} {d['unit']}")
+    return out
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -922,6 +967,8 @@ def main():
     p.add_argument("--no-plain", action="store_true",
                    help="dense / batch: skip timing the plain kernel (popcount / one call per pair)")
     p.add_argument("--dtype", choices=["int8", "fp8"], default="int8", help="dense: tensor-core operand type")
+    p.add_argument("--no-extras", action="store_true",
+                   help="SISI at N=1: skip the short runs of the other workloads added to the line")
     args = p.parse_args()
     if args.warmup < 3:
         p.error("--warmup must be >= 3")
