@@ -88,6 +88,16 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+# DRAM bytes (read + write) per launch of the dominant kernel, from ncu
+# captures summarised in profiles/: the 2^25 x 2^25 capture of the tile kernel
+# (268.73 MB read + 13.22 MB written) scaled by 8 to the 2^28 x 2^28 launch
+# (tiles, inputs and matches all grow in proportion).
+TRAFFIC_PER_LAUNCH = {
+    "ip/sisi_large/out": 8 * (268.727808e6 + 13.220096e6),
+    "ip/sisi_mid/out": 268.727808e6 + 13.220096e6,
+}
+
+
 # ----------------------------------------------------------------- inputs --
 def make_pair(name: str):
     from set_intersection_b200 import generate
@@ -364,10 +374,7 @@ def run_ours(args, rank: int, world: int):
     alg_bytes = 4 * (n_a + n_b) + (4 * c if args.materialize else 0)
     tile_avg_ms = tile_ms.value / max(1, tile_n.value)
     achieved = alg_bytes / (tile_avg_ms * 1e-3) / 1e9 if tile_n.value else None
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        traffic = json.load(open(tf)).get(f"{args.technique}/{args.workload}/{'out' if args.materialize else 'count'}")
+    traffic = TRAFFIC_PER_LAUNCH.get(f"{args.technique}/{args.workload}/{'out' if args.materialize else 'count'}")
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
