@@ -657,6 +657,10 @@ def run_ours_dense(args, rank: int, world: int):
                 "avg_launch_ms": avg_ms, "launches": int(k_n.value),
                 "peak_source": ("2 x measured dense bf16 (8-bit operands run at twice the 16-bit rate)"
                                 if "bf16_tflops" in peaks else "2 x fallback bf16")}
+        i8 = cublas_int8_tops(dev) if not args.no_plain else None
+        if i8:
+            roof["cublas_int8_tops_measured"] = i8
+            roof["frac_of_cublas_int8"] = achieved / i8
     elif powerlaw:
         # algorithmic bytes: every pair reads its smaller set once (4 B per
         # probe), each set is read once more as the staged side, and every
@@ -704,6 +708,32 @@ def run_ours_dense(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def cublas_int8_tops(dev, n: int = 8192, reps: int = 10):
+    """cuBLAS's own dense INT8 GEMM (torch._int_mm, s32 accumulation) on this
+    GPU, best of `reps` CUDA-event-timed runs of an n^3 product: an 8-bit
+    denominator measured beside the kernel."""
+    import torch
+    try:
+        a = torch.randint(-3, 4, (n, n), dtype=torch.int8, device=dev)
+        b = torch.randint(-3, 4, (n, n), dtype=torch.int8, device=dev)
+        for _ in range(3):
+            torch._int_mm(a, b)
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        del a, b
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    except Exception as e:  # not fatal: the bf16-derived peak stands
+        log(f"cuBLAS int8 measurement unavailable: {e}")
+        return None
 
 
 # ------------------------------------------------------------ batched pairs --
