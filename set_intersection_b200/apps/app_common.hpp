@@ -25,6 +25,7 @@
 #include <map>
 #include <set>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "si.h"
@@ -161,6 +162,79 @@ inline void box(const char* title, const std::vector<std::pair<std::string, std:
     std::printf("└───────────────────────────────────────────────────┘\n");
 }
 
+// Result text (include/io.hpp:91-136): "(i,j): count\n", 1-based, formatted by
+// hand into a large buffer and written in big blocks.  Runs are formatted on
+// a writer thread while the GPU computes the next run.
+class ResultWriter {
+  public:
+    bool open(const std::string& path) {
+        f_ = std::fopen(path.c_str(), "w");
+        buf_.resize(kBuf);
+        return f_ != nullptr;
+    }
+    ~ResultWriter() { close(); }
+    void close() {
+        join();
+        if (f_) {
+            flush();
+            std::fclose(f_);
+            f_ = nullptr;
+        }
+    }
+    // all pairs of one run, in the reference's loop order; their counts are
+    // rc[tri(k, i, j)] when k > 0 (the whole collection's triangle), else the
+    // run's own layout (self: tri(stride, i - A, j - A), cross: (i - A) * stride + (j - B))
+    void run_async(const Tile& A, const Tile& B, const uint32_t* rc, uint64_t stride, uint64_t k = 0) {
+        join();
+        worker_ = std::thread([this, A, B, rc, stride, k] {
+            const bool self = A.id == B.id;
+            for (uint32_t i = A.start; i < A.end; ++i)
+                for (uint32_t j = self ? i + 1 : B.start; j < B.end; ++j)
+                    line(i, j, rc[k ? tri(k, i, j)
+                                    : self ? tri(stride, i - A.start, j - A.start)
+                                           : uint64_t(i - A.start) * stride + (j - B.start)]);
+        });
+    }
+    void join() {
+        if (worker_.joinable()) worker_.join();
+    }
+
+  private:
+    static constexpr size_t kBuf = 8u << 20;
+    static char* put(char* p, uint32_t v) {
+        char t[10];
+        int n = 0;
+        do {
+            t[n++] = static_cast<char>('0' + v % 10);
+            v /= 10;
+        } while (v);
+        while (n) *p++ = t[--n];
+        return p;
+    }
+    void line(uint32_t i, uint32_t j, uint32_t c) {
+        if (used_ + 48 > kBuf) flush();
+        char* p = buf_.data() + used_;
+        *p++ = '(';
+        p = put(p, i + 1);
+        *p++ = ',';
+        p = put(p, j + 1);
+        *p++ = ')';
+        *p++ = ':';
+        *p++ = ' ';
+        p = put(p, c);
+        *p++ = '\n';
+        used_ = static_cast<size_t>(p - buf_.data());
+    }
+    void flush() {
+        if (used_) std::fwrite(buf_.data(), 1, used_, f_);
+        used_ = 0;
+    }
+    FILE* f_ = nullptr;
+    std::vector<char> buf_;
+    size_t used_ = 0;
+    std::thread worker_;
+};
+
 enum class Kind { Sorted, Dense };
 
 struct Spec {
@@ -241,6 +315,15 @@ inline int run(const Spec& spec, int argc, char** argv) {
     lap("Transfer to device");
 
     const auto runs = tile_pairs(k, a.partition);
+    ResultWriter out;
+    if (!a.output.empty()) {
+        std::printf("Writing result to file %s\n", a.output.c_str());
+        if (!out.open(a.output)) {
+            std::printf("cannot write %s\n", a.output.c_str());
+            return 1;
+        }
+    }
+    bool streamed = false;  // the result lines were written run by run
     if (k == 2 && spec.kind == Kind::Sorted) {
         // one pair: the single-pair path
         const size_t ws_bytes = si_sisi_workspace_size(d.sizes[0], d.sizes[1], spec.tech);
@@ -288,7 +371,8 @@ inline int run(const Spec& spec, int argc, char** argv) {
         cudaFree(d_counts);
     }
     if (k >= 2 && !dense_done && !(k == 2 && spec.kind == Kind::Sorted)) {
-        // run by run, as the reference: each tile pair's counts, then copied into the triangle
+        // run by run, as the reference; each run's lines are formatted on the
+        // writer thread while the next run computes (two host buffers)
         const uint32_t stride = runs.size() == 1 ? k : a.partition;
         const size_t ws_bytes = si_misi_workspace_size({0, std::min(k, a.partition)}, {0, std::min(k, a.partition)},
                                                        sorted_tech) +
@@ -300,28 +384,28 @@ inline int run(const Spec& spec, int argc, char** argv) {
         uint32_t* d_counts = nullptr;
         SI_APP_CUDA(cudaMalloc(&ws, ws_bytes));
         SI_APP_CUDA(cudaMalloc(&d_counts, run_counts * 4));
-        std::vector<uint32_t> rc(run_counts);
+        std::vector<uint32_t> rc[2] = {std::vector<uint32_t>(run_counts), std::vector<uint32_t>(run_counts)};
         double t_int = 0, t_res = 0;
+        int cur = 0;
         for (auto& run : runs) {
             const Tile& A = run.first;
             const Tile& B = run.second;
-            const bool self = A.id == B.id;
             auto r0 = std::chrono::steady_clock::now();
             SI_APP_TRY(si_misi(d_el, d_off, {A.start, A.end}, {B.start, B.end}, stride, sorted_tech, d_counts, ws,
                                ws_bytes, nullptr));
             SI_APP_TRY(si_workspace_check(ws, nullptr));
             auto r1 = std::chrono::steady_clock::now();
-            SI_APP_CUDA(cudaMemcpy(rc.data(), d_counts, run_counts * 4, cudaMemcpyDeviceToHost));
+            SI_APP_CUDA(cudaMemcpy(rc[cur].data(), d_counts, run_counts * 4, cudaMemcpyDeviceToHost));
             auto r2 = std::chrono::steady_clock::now();
-            for (uint32_t i = A.start; i < A.end; ++i)
-                for (uint32_t j = self ? i + 1 : B.start; j < B.end; ++j) {
-                    const uint64_t idx = self ? tri(stride, i - A.start, j - A.start)
-                                              : uint64_t(i - A.start) * stride + (j - B.start);
-                    counts[tri(k, i, j)] = rc[idx];
-                }
+            if (!a.output.empty()) {
+                out.run_async(A, B, rc[cur].data(), stride);  // waits for the run before the previous one
+                cur ^= 1;
+            }
             t_int += std::chrono::duration<double, std::milli>(r1 - r0).count();
             t_res += std::chrono::duration<double, std::milli>(r2 - r1).count();
         }
+        out.join();
+        streamed = true;
         timings.push_back({"Intersection", t_int});
         timings.push_back({"Transfer result", t_res});
         t0 = std::chrono::steady_clock::now();
@@ -345,25 +429,15 @@ inline int run(const Spec& spec, int argc, char** argv) {
     box("────────────────Timings (in ms)────────────────────", rows);
 
     if (!a.output.empty()) {
-        std::printf("Writing result to file %s\n", a.output.c_str());
-        FILE* f = std::fopen(a.output.c_str(), "w");
-        if (!f) {
-            std::printf("cannot write %s\n", a.output.c_str());
-            return 1;
-        }
-        // include/io.hpp:91-136: one run in row-major order, else run by run
-        if (runs.size() <= 1) {
-            for (uint32_t i = 0; i < k; ++i)
-                for (uint32_t j = i + 1; j < k; ++j) std::fprintf(f, "(%u,%u): %u\n", i + 1, j + 1, counts[tri(k, i, j)]);
-        } else {
+        // the whole-collection counts (single pair, dense path) follow the
+        // runs' order: a run is a self tile or a cross tile of the triangle
+        if (!streamed && k >= 2) {
             for (auto& run : runs) {
-                const bool self = run.first.id == run.second.id;
-                for (uint32_t i = run.first.start; i < run.first.end; ++i)
-                    for (uint32_t j = self ? i + 1 : run.second.start; j < run.second.end; ++j)
-                        std::fprintf(f, "(%u,%u): %u\n", i + 1, j + 1, counts[tri(k, i, j)]);
+                out.run_async(run.first, run.second, counts.data(), 0, k);
+                out.join();
             }
         }
-        std::fclose(f);
+        out.close();
         std::printf("Finished\n");
     }
     return 0;

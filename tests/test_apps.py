@@ -13,11 +13,12 @@ from set_intersection_b200 import dataset as fmt
 
 BIN = os.path.join(ROOT, "set_intersection_b200", "bin")
 APPS = ["ip", "obs", "hi", "bitmap_dynamic", "bitmap_naive", "matrix_multiplication"]
+TOOLS = ["txt2bin", "bin2txt"]
 
 
 @pytest.fixture(scope="module")
 def apps():
-    if not all(os.access(os.path.join(BIN, a), os.X_OK) for a in APPS):
+    if not all(os.access(os.path.join(BIN, a), os.X_OK) for a in APPS + TOOLS):
         subprocess.run(["make", "-C", os.path.join(ROOT, "set_intersection_b200"), "apps"], check=True,
                        capture_output=True)
     return BIN
@@ -79,3 +80,34 @@ def test_launch_geometry_flags_are_accepted(cuda, apps, tmp_path):
             "128", "--buckets", "7", "--bucket-size", "9", "--warp", "--path")
     assert r.returncode == 0, r.stdout
     assert out.read_text() == open(golden_path("misi_mixed.std.txt")).read()
+
+
+def test_txt2bin_and_bin2txt_match_the_reference_tools(apps, tmp_path):
+    """Byte-identical to the reference's own txt2bin / bin2txt outputs
+    (tests/golden/text_sets_*.bin were made by them)."""
+    r = run("txt2bin", golden_path("text_sets.txt"), str(tmp_path / "x"))
+    assert r.returncode == 0, r.stdout
+    assert (tmp_path / "x_asc.bin").read_bytes() == open(golden_path("text_sets_asc.bin"), "rb").read()
+    assert (tmp_path / "x_desc.bin").read_bytes() == open(golden_path("text_sets_desc.bin"), "rb").read()
+    r = run("bin2txt", golden_path("text_sets_asc.bin"), str(tmp_path / "y"))
+    assert r.returncode == 0, r.stdout
+    ds = fmt.read_dataset(golden_path("text_sets_asc.bin"))
+    want = "".join("".join(f"{v} " for v in s) + "\n" for s in ds.sets())
+    assert (tmp_path / "y.txt").read_text() == want
+
+
+@pytest.mark.parametrize("text,msg", [("1 2 3\n5 4\n", "not strictly increasing"), ("1 2 2\n", "not strictly"),
+                                      ("1 x 3\n", "not a 32-bit"), ("4294967296\n", "not a 32-bit"),
+                                      ("-1 2\n", "not a 32-bit")])
+def test_txt2bin_rejects_bad_sets(apps, tmp_path, text, msg):
+    src = tmp_path / "bad.txt"
+    src.write_text(text)
+    r = run("txt2bin", str(src), str(tmp_path / "o"))
+    assert r.returncode == 1 and msg in r.stdout
+
+
+def test_bin2txt_rejects_truncated_file(apps, tmp_path):
+    raw = open(golden_path("text_sets_asc.bin"), "rb").read()
+    (tmp_path / "t.bin").write_bytes(raw[:-1])
+    r = run("bin2txt", str(tmp_path / "t.bin"), str(tmp_path / "o"))
+    assert r.returncode == 1
