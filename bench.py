@@ -320,6 +320,12 @@ def run_ours(args, rank: int, world: int):
     ms_total = start.elapsed_time(stop)
     tile_ms, tile_n = ctypes.c_double(0), ctypes.c_uint64(0)
     lib.si_timer_read(b"sisi_tile", ctypes.byref(tile_ms), ctypes.byref(tile_n))
+    phases = {}
+    for ph in ("sisi_prepare", "sisi_split", "sisi_tile", "sisi_scan", "sisi_copy"):
+        p_ms, p_n = ctypes.c_double(0), ctypes.c_uint64(0)
+        lib.si_timer_read(ph.encode(), ctypes.byref(p_ms), ctypes.byref(p_n))
+        if p_n.value:
+            phases[ph] = p_ms.value / p_n.value
     lib.si_timer_reset()
     ws.check(stream)
     torch.cuda.synchronize()
@@ -398,7 +404,8 @@ def run_ours(args, rank: int, world: int):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": f"ip_tile_kernel<{'bitmap probe' if args.technique in ('bitmap', 'auto') else 'merge path'}>", "alg_bytes_per_launch": alg_bytes,
-                     "avg_launch_ms": tile_avg_ms, "launches": int(tile_n.value), "peak_source": peak_src},
+                     "avg_launch_ms": tile_avg_ms, "launches": int(tile_n.value), "peak_source": peak_src,
+                     "phase_avg_ms": phases},
         "e2e": e2e,
         "gpu_launches": 3 * args.steps,
         "clocks": clocks.summary(),

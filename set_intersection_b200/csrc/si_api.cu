@@ -129,10 +129,11 @@ size_t si_sisi_workspace_size(uint64_t nA, uint64_t nB, si_technique t) {
     switch (t) {
         case SI_TECH_IP:
         case SI_TECH_HI:
-        case SI_TECH_BITMAP:
             return si::ip_workspace_size(nA, nB);
+        case SI_TECH_BITMAP:
+            return si::ip_workspace_size(nA, nB, 1);
         case SI_TECH_AUTO:
-            return std::max(si::ip_workspace_size(nA, nB), si::obs_workspace_size(nA, nB));
+            return std::max(si::ip_workspace_size(nA, nB, 1), si::obs_workspace_size(nA, nB));
         case SI_TECH_OBS:
             return si::obs_workspace_size(nA, nB);
         default:
