@@ -14,7 +14,8 @@ of each line under "other_workloads" (--no-extras skips them).
 
 One "step" is one pass of the single-pair (SISI) hot path over one pair of
 sets: the workload by default is |A| = |B| = 2^28 sorted unique uint32 drawn
-from [0, 2^31), intersect-path technique, count + materialised elements.
+from [0, 2^31), technique auto (for two sets of similar size: the bitmap
+engine over value-pivot tiles), count + materialised elements.
 Metric: Gelem/s = (|A| + |B|) / step time.
 
   value   device-timed (CUDA events on the launching stream), inputs resident
@@ -22,7 +23,8 @@ Metric: Gelem/s = (|A| + |B|) / step time.
   e2e     the same metric through the public host API (api.intersect_host):
           pinned host sets -> H2D -> kernels -> count + elements D2H, per step.
   roofline  live per-launch time of the dominant kernel (the tile kernel) from the
-          library's phase timer over the timed region, against measured HBM.
+          library's phase timer over the timed region, against measured HBM;
+          phase_avg_ms lists every phase of the step (split, tiles, scan, copy).
   cpu_baseline  the reference's own CPU executable (oracle/_ref/stdintersection,
           built from the reference sources) on a bounded sample of the same
           workload, timed by the reference's HostTimer.
@@ -92,6 +94,8 @@ def log(*a):
 # captures summarised in profiles/: the 2^25 x 2^25 capture of the tile kernel
 # (268.73 MB read + 13.22 MB written) scaled by 8 to the 2^28 x 2^28 launch
 # (tiles, inputs and matches all grow in proportion).
+SKEW_RATIO = 64  # SI_TECH_AUTO: obs when one set is more than this many times the other
+
 TRAFFIC_PER_LAUNCH = {
     "ip/sisi_large/out": 8 * (268.727808e6 + 13.220096e6),
     "ip/sisi_mid/out": 268.727808e6 + 13.220096e6,
@@ -321,7 +325,8 @@ def run_ours(args, rank: int, world: int):
     tile_ms, tile_n = ctypes.c_double(0), ctypes.c_uint64(0)
     lib.si_timer_read(b"sisi_tile", ctypes.byref(tile_ms), ctypes.byref(tile_n))
     phases = {}
-    for ph in ("sisi_prepare", "sisi_split", "sisi_tile", "sisi_scan", "sisi_copy"):
+    for ph in ("sisi_prepare", "sisi_split", "sisi_tile", "sisi_scan", "sisi_copy", "obs_sample", "obs_search",
+               "obs_scan", "obs_compact"):
         p_ms, p_n = ctypes.c_double(0), ctypes.c_uint64(0)
         lib.si_timer_read(ph.encode(), ctypes.byref(p_ms), ctypes.byref(p_n))
         if p_n.value:
@@ -378,9 +383,24 @@ def run_ours(args, rank: int, world: int):
     peak = peaks.get("hbm_gbs", FALLBACK_HBM_GBS)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     alg_bytes = 4 * (n_a + n_b) + (4 * c if args.materialize else 0)
-    tile_avg_ms = tile_ms.value / max(1, tile_n.value)
-    achieved = alg_bytes / (tile_avg_ms * 1e-3) / 1e9 if tile_n.value else None
-    traffic = TRAFFIC_PER_LAUNCH.get(f"{args.technique}/{args.workload}/{'out' if args.materialize else 'count'}")
+    # the engine that ran: auto searches a much smaller set in the larger (obs)
+    # and streams pairs of similar size through the bitmap tiles
+    engine = args.technique
+    if engine == "auto":
+        engine = "obs" if min(n_a, n_b) * SKEW_RATIO < max(n_a, n_b) else "bitmap"
+    kernel, launches = {
+        "ip": ("ip_tile_kernel<merge path>", 3),
+        "hi": ("ip_tile_kernel<hash probe>", 3),
+        "bitmap": ("bm_stage_kernel", 7 if args.materialize else 3),
+        "obs": ("obs_search_kernel", 4 if args.materialize else 2),
+    }[engine]
+    if engine == "obs":
+        tile_avg_ms = phases.get("obs_search")
+        achieved = None  # dependent-load chains over a fraction of the larger set: latency-bound
+    else:
+        tile_avg_ms = tile_ms.value / max(1, tile_n.value)
+        achieved = alg_bytes / (tile_avg_ms * 1e-3) / 1e9 if tile_n.value else None
+    traffic = TRAFFIC_PER_LAUNCH.get(f"{engine}/{args.workload}/{'out' if args.materialize else 'count'}")
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -403,11 +423,11 @@ def run_ours(args, rank: int, world: int):
                    "parallelism": f"replicas{world}", "parity_vs_oracle": parity},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": f"ip_tile_kernel<{'bitmap probe' if args.technique in ('bitmap', 'auto') else 'merge path'}>", "alg_bytes_per_launch": alg_bytes,
+                     "kernel": kernel, "engine": engine, "alg_bytes_per_launch": alg_bytes,
                      "avg_launch_ms": tile_avg_ms, "launches": int(tile_n.value), "peak_source": peak_src,
                      "phase_avg_ms": phases},
         "e2e": e2e,
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": launches * args.steps,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
     }
@@ -1002,7 +1022,7 @@ def main():
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload", choices=sorted(WORKLOADS), default="sisi_large")
-    p.add_argument("--technique", default="ip")
+    p.add_argument("--technique", default="auto")
     p.add_argument("--count-only", dest="materialize", action="store_false")
     p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--no-e2e", action="store_true")

@@ -15,13 +15,18 @@
 //    split across tiles (no "augmentation" atomic, quirk of
 //    include/helpers.cuh:121-124).
 //  * Staging: each tile's A and B ranges are copied into shared memory by the
-//    bulk-copy (TMA) engine, 16-byte aligned middle + <= 3 ragged elements per
-//    edge by plain loads; every input byte is read from HBM once.
+//    bulk-copy (TMA) engine as their 16-byte aligned supersets (every block
+//    copied holds an element of the range); every input byte is read from HBM
+//    once.
 //  * Thread level: merge-path split per thread in shared memory with one
 //    tie rule (A first on ties), then a sentinel-terminated serial merge.
 //  * Output: matches are compacted per tile and placed with a decoupled
 //    look-back over tile aggregates (single pass); count-only mode instead
 //    accumulates tile counts into 256 spread partial sums.
+//
+// Technique bitmap (and auto for pairs of similar size) shares the pivot
+// split (S = 16384) and then runs its own engine, bm_stage_kernel: two
+// bitmaps per tile AND-ed, per-tile counts, a scan and a copy (no look-back).
 #include <algorithm>
 #include <cub/device/device_scan.cuh>
 
@@ -186,19 +191,17 @@ constexpr int kCtasPerSm = 2;
 constexpr int kSlots = 8;
 constexpr int kOutQ = 16;                    // output descriptors in flight
 constexpr int kGroup = 4;                    // consecutive tiles per scheduling unit (one look-back each)
-constexpr uint32_t kInRing = 14336;          // u32: 56 KiB (the merge path adds the bitmap area: 72 KiB)
+constexpr uint32_t kInRing = 14336;          // u32: 56 KiB (the merge path adds the table's area: 72 KiB)
 constexpr uint32_t kOutRing = 8192;          // u32: 32 KiB, a power of two
-constexpr uint32_t kBitmapSmemWords = 2048;  // u32 per bitmap buffer (8 KiB); two buffers
 constexpr uint32_t kHashSlots = 4096;        // open-addressing table (16 KiB): load factor <= 1/2
-// Shared memory after the rings: two bitmaps (bitmap probe) or one hash table (hash probe).
-// Input ring of an inner loop: the merge path needs no bitmaps, so its ring
-// takes their space (about three average tiles instead of two).
+// Shared memory after the rings: the hash table (hash probe).  The merge path
+// needs no table, so its input ring takes that space (about three average
+// tiles instead of two).
 __host__ __device__ constexpr uint32_t in_ring_words(int inner) {
-    return inner == 0 ? kInRing + 2 * kBitmapSmemWords : kInRing;
+    return inner == 0 ? kInRing + kHashSlots : kInRing;
 }
 __host__ __device__ constexpr size_t smem_bytes(int inner) {
-    return size_t(in_ring_words(inner) + kOutRing + (inner == 2 ? kHashSlots : inner == 1 ? 2 * kBitmapSmemWords : 0)) *
-           sizeof(uint32_t);
+    return size_t(in_ring_words(inner) + kOutRing + (inner == 2 ? kHashSlots : 0)) * sizeof(uint32_t);
 }
 static_assert((kOutRing & (kOutRing - 1)) == 0, "output ring is indexed modulo its size");
 static_assert(kS <= kOutRing, "one tile's matches must fit the output ring");
@@ -285,6 +288,7 @@ __device__ __forceinline__ uint64_t look_back(uint64_t* status, uint64_t t, uint
 // owns as a bit mask over a contiguous run of one staged set: the matched
 // values are src[start + x] for every set bit x, in ascending order, and the
 // runs of consecutive threads are consecutive.
+// (kBitmapProbe selects the separate bitmap engine, bm_stage_kernel, below.)
 enum Inner { kMergePath = 0, kBitmapProbe = 1, kHashProbe = 2 };
 
 struct ThreadMatches {
@@ -344,51 +348,6 @@ __device__ __forceinline__ ThreadMatches merge_inner(const uint32_t* sA, int na,
         }
     }
     return {sA, i0, mask};
-}
-
-// Bitmap probe (the reference's bitmap_dynamic, src/bitmap_dynamic.cu:240-276,
-// restricted to one tile): the set part with the narrower value span is
-// written as a bitmap of that span into shared memory, the other part probes
-// it.  A tile only holds the values between two pivots, so the span is small
-// for all but very sparse data; a tile whose span exceeds the bitmap falls
-// back to the merge path.  Two bitmap buffers alternate between bitmap tiles:
-// a buffer's words are cleared right before its next use, after the other
-// buffer's tile has passed two barriers, so no thread still probes them.
-constexpr uint32_t kBitmapWords = kBitmapSmemWords;  // a span of up to 65536 values
-__device__ __forceinline__ bool bitmap_fits(const uint32_t* sA, int na, const uint32_t* sB, int nb, bool& buildA,
-                                            uint32_t& span) {
-    if (na == 0 || nb == 0) return false;
-    const uint32_t spanA = sA[na - 1] - sA[0], spanB = sB[nb - 1] - sB[0];
-    buildA = spanA <= spanB;
-    span = buildA ? spanA : spanB;
-    return span < kBitmapWords * 32u;
-}
-
-__device__ __forceinline__ ThreadMatches bitmap_inner(const uint32_t* sA, int na, const uint32_t* sB, int nb,
-                                                      bool buildA, uint32_t span, int tid, uint32_t* bm,
-                                                      uint32_t stale_words) {
-    for (uint32_t w = tid; w < stale_words; w += kConsumers) bm[w] = 0u;
-    named_barrier(kConsumerBar, kConsumers);
-    const uint32_t* X = buildA ? sA : sB;
-    const uint32_t* Y = buildA ? sB : sA;
-    const int nx = buildA ? na : nb, ny = buildA ? nb : na;
-    const uint32_t base = X[0];
-#pragma unroll 4
-    for (int e = tid; e < nx; e += kConsumers) {
-        const uint32_t v = X[e] - base;
-        if (v <= span) atomicOr(bm + (v >> 5), 1u << (v & 31));  // always, for sorted input
-    }
-    named_barrier(kConsumerBar, kConsumers);
-    const int r = ((ny + kConsumers - 1) / kConsumers) | 1;  // <= 15: one part holds <= kS values
-    const int j0 = min(tid * r, ny), j1 = min(j0 + r, ny);
-    uint64_t mask = 0;
-#pragma unroll 4
-    for (int e = j0; e < j1; ++e) {
-        const uint32_t v = Y[e] - base;
-        const uint32_t w = v <= span ? bm[v >> 5] : 0u;
-        mask |= static_cast<uint64_t>((w >> (v & 31)) & 1u) << (e - j0);
-    }
-    return {Y, j0, mask};
 }
 
 // Hash probe (the reference's hi, src/hi.cu:295-479, restricted to one tile):
@@ -456,7 +415,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     uint32_t* in_ring = smem;
     constexpr uint32_t kRing = in_ring_words(kInner);
     uint32_t* out_ring = smem + kRing;
-    uint32_t* bitmaps = smem + kRing + kOutRing;  // 2 x kBitmapSmemWords (bitmap) or the hash table
+    uint32_t* table = smem + kRing + kOutRing;  // hash probe: the hash table
     __shared__ __align__(8) uint64_t full[kSlots], empty[kSlots], ofull[kOutQ], oempty[kOutQ];
     __shared__ __align__(8) uint64_t s_released_out;  // output ring: virtual offset written out so far
     __shared__ uint32_t s_otile[kOutQ], s_ocount[kOutQ];
@@ -468,9 +427,6 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
 
     uint32_t* err = reinterpret_cast<uint32_t*>(ws);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if constexpr (kInner == kBitmapProbe) {
-        for (uint32_t w = tid; w < 2 * kBitmapSmemWords; w += kBlock) bitmaps[w] = 0u;
-    }
     if (tid == 0) {
         for (int i = 0; i < kSlots; ++i) {
             mbar_init(&full[i], 1);
@@ -652,8 +608,6 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     // ---------------------------------------------------------- consumers --
     uint64_t my_count = 0;     // count-only: this thread's matches over all its tiles
     uint64_t ohead = 0;        // element output: virtual output-ring head (same in every thread)
-    uint32_t stale0 = 0u, stale1 = 0u;  // bitmap words left set in each buffer
-    uint32_t nbm = 0;          // bitmap tiles so far (buffer parity)
     uint32_t k = 0;            // tiles consumed so far
     for (;; ++k) {
         const uint32_t slot = k % kSlots;
@@ -663,16 +617,8 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
         const uint32_t* sA = in_ring + d.offA;
         const uint32_t* sB = in_ring + d.offB;
         ThreadMatches tm;
-        bool buildA = true;
-        uint32_t span = 0;
         if (kInner == kHashProbe && d.na > 0 && d.nb > 0 && min(d.na, d.nb) <= static_cast<int>(kHashSlots / 2)) {
-            tm = hash_inner(sA, d.na, sB, d.nb, tid, bitmaps, &s_has_max, !kOut);
-        } else if (kInner == kBitmapProbe && bitmap_fits(sA, d.na, sB, d.nb, buildA, span)) {
-            const uint32_t buf = nbm & 1u;
-            tm = bitmap_inner(sA, d.na, sB, d.nb, buildA, span, tid, bitmaps + buf * kBitmapSmemWords,
-                              buf ? stale1 : stale0);
-            if (buf) stale1 = (span >> 5) + 1; else stale0 = (span >> 5) + 1;
-            ++nbm;
+            tm = hash_inner(sA, d.na, sB, d.nb, tid, table, &s_has_max, !kOut);
         } else {
             tm = merge_inner(sA, d.na, sB, d.nb, d.fast != 0, tid);
         }
@@ -783,7 +729,6 @@ constexpr uint32_t kBmWords = 4096;             // per bitmap: a range of up to 
 constexpr uint32_t kBmRing = 40960;             // u32: 160 KiB, about 2.5 tiles of 2 x 8192 elements
 constexpr int kBmSlots = 8;
 constexpr uint32_t kBmBar = 1;                  // named barrier of the 31 warps
-constexpr uint32_t kBmWordsPerThread = (kBmWords + kBmConsumers - 1) / kBmConsumers;
 constexpr uint32_t kBmYPerThread = (kBmS + kBmConsumers - 1) / kBmConsumers;  // search fallback
 constexpr size_t kBmSmem = size_t(4 * kBmWords + kBmRing) * sizeof(uint32_t);
 static_assert(2 * (kBmS + 4) <= kBmRing, "one tile's aligned supersets must fit the ring");
@@ -797,34 +742,44 @@ struct BmDesc {
     uint32_t nx, ny;
 };
 
-// Sets the bit of every value of a staged part that lies in [lo, lo + span]:
-// 16-byte groups of the staged superset, group g holding elements
-// 4 g - mis ... 4 g - mis + 3.  Only the first and the last group hold words
-// outside [0, n); they go through a checked path, the interior groups through
-// one predicated shared atomic OR per value.
+// Sets the bits of the values of both staged parts that lie in [lo, lo + span].
+// A part is read as 16-byte groups of its staged superset, group g holding
+// elements 4 g - mis ... 4 g - mis + 3.  Only a part's first and last group hold
+// words outside [0, n); four threads take those through a checked path.  The
+// interior groups of both parts form one index space dealt round-robin over
+// the threads (one predicated shared atomic OR per value), so every thread
+// gets the same number of groups to within one.
 __device__ __forceinline__ void bm_set(uint32_t* bm, uint32_t o, uint32_t span) {
     if (o <= span) atomicOr(bm + (o >> 5), 1u << (o & 31));
 }
-__device__ __forceinline__ void bm_build(const uint32_t* s, uint32_t mis, uint32_t n, uint32_t lo, uint32_t span,
-                                         uint32_t* bm, int tid) {
-    const uint4* g4 = reinterpret_cast<const uint4*>(s - mis);
-    const uint32_t ngroups = (n + mis + 3) / 4;
-    if (tid < 2 && ngroups > 0) {
-        const uint32_t g = tid == 0 ? 0u : ngroups - 1;
-        if (tid == 0 || ngroups > 1) {
-            const uint4 v4 = g4[g];
-            const uint32_t vv[4] = {v4.x, v4.y, v4.z, v4.w};
-            const int e0 = static_cast<int>(4 * g) - static_cast<int>(mis);
+__device__ __forceinline__ void bm_edge(const uint32_t* s, uint32_t mis, uint32_t n, uint32_t lo, uint32_t span,
+                                        uint32_t* bm, uint32_t g) {
+    const uint4 v4 = reinterpret_cast<const uint4*>(s - mis)[g];
+    const uint32_t vv[4] = {v4.x, v4.y, v4.z, v4.w};
+    const int e0 = static_cast<int>(4 * g) - static_cast<int>(mis);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int e = e0 + q;
-                if (e >= 0 && e < static_cast<int>(n)) bm_set(bm, vv[q] - lo, span);
-            }
-        }
+    for (int q = 0; q < 4; ++q) {
+        const int e = e0 + q;
+        if (e >= 0 && e < static_cast<int>(n)) bm_set(bm, vv[q] - lo, span);
     }
+}
+__device__ __forceinline__ void bm_build(const uint32_t* sx, uint32_t misX, uint32_t nx, uint32_t* bx,
+                                         const uint32_t* sy, uint32_t misY, uint32_t ny, uint32_t* by, uint32_t lo,
+                                         uint32_t span, int tid) {
+    const uint32_t ngx = (nx + misX + 3) / 4, ngy = (ny + misY + 3) / 4;
+    // the edge groups go to the last threads, which get no more interior groups than the others
+    if (tid == kBmConsumers - 1 && ngx > 0) bm_edge(sx, misX, nx, lo, span, bx, 0);
+    if (tid == kBmConsumers - 2 && ngx > 1) bm_edge(sx, misX, nx, lo, span, bx, ngx - 1);
+    if (tid == kBmConsumers - 3 && ngy > 0) bm_edge(sy, misY, ny, lo, span, by, 0);
+    if (tid == kBmConsumers - 4 && ngy > 1) bm_edge(sy, misY, ny, lo, span, by, ngy - 1);
+    const uint32_t ix = ngx > 2 ? ngx - 2 : 0u, iy = ngy > 2 ? ngy - 2 : 0u;
+    const uint4* gx = reinterpret_cast<const uint4*>(sx - misX) + 1;
+    const uint4* gy = reinterpret_cast<const uint4*>(sy - misY) + 1;
 #pragma unroll 2
-    for (uint32_t g = 1 + tid; g + 1 < ngroups; g += kBmConsumers) {
-        const uint4 v4 = g4[g];
+    for (uint32_t c = tid; c < ix + iy; c += kBmConsumers) {
+        const bool isx = c < ix;
+        const uint4 v4 = *(isx ? gx + c : gy + (c - ix));
+        uint32_t* bm = isx ? bx : by;
         bm_set(bm, v4.x - lo, span);
         bm_set(bm, v4.y - lo, span);
         bm_set(bm, v4.z - lo, span);
@@ -979,13 +934,13 @@ __global__ void __launch_bounds__(kBmBlock, 1) bm_stage_kernel(
         // the pass over tile k - 2, which every warp finished before it
         // arrived at the barrier of tile k - 1 below.
         // this thread's hits: bits of its words (bitmaps) or of its Y run (search)
-        const uint32_t w0 = min(words, tid * kBmWordsPerThread), w1 = min(words, w0 + kBmWordsPerThread);
+        const uint32_t wpt = (words + kBmConsumers - 1) / kBmConsumers;
+        const uint32_t w0 = min(words, tid * wpt), w1 = min(words, w0 + wpt);
         const uint32_t yrun = (ny + kBmConsumers - 1) / kBmConsumers;  // <= kBmYPerThread
         const uint32_t j0 = min(ny, tid * yrun), j1 = min(ny, j0 + yrun);
         uint32_t ymask = 0;
         if (fits) {
-            bm_build(sx, d.misX, nx, lo, span, bx, tid);
-            bm_build(sy, d.misY, ny, lo, span, by, tid);
+            bm_build(sx, d.misX, nx, bx, sy, d.misY, ny, by, lo, span, tid);
         } else if (any) {
             for (uint32_t j = j0; j < j1; ++j) {
                 const uint32_t v = sy[j];
