@@ -90,15 +90,18 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-# DRAM bytes (read + write) per launch of the dominant kernel, from ncu
-# captures summarised in profiles/: the 2^25 x 2^25 capture of the tile kernel
-# (268.73 MB read + 13.22 MB written) scaled by 8 to the 2^28 x 2^28 launch
-# (tiles, inputs and matches all grow in proportion).
 SKEW_RATIO = 64  # SI_TECH_AUTO: obs when one set is more than this many times the other
 
+# DRAM bytes (read + write) per launch of the dominant kernel, from ncu
+# captures summarised in profiles/: the 2^25 x 2^25 captures of the ip tile
+# kernel (268.73 MB read + 13.22 MB written) and of the bitmap engine's
+# bm_stage_kernel (268.64 MB + 14.60 MB), scaled by 8 to the 2^28 x 2^28 launch
+# (tiles, inputs and matches all grow in proportion).
 TRAFFIC_PER_LAUNCH = {
     "ip/sisi_large/out": 8 * (268.727808e6 + 13.220096e6),
     "ip/sisi_mid/out": 268.727808e6 + 13.220096e6,
+    "bitmap/sisi_large/out": 8 * (268.642816e6 + 14.604288e6),
+    "bitmap/sisi_mid/out": 268.642816e6 + 14.604288e6,
 }
 
 
