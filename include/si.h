@@ -74,9 +74,12 @@ const char* si_last_error_string(void);
  * count; element output is this engine's addition, ordered as
  * std::set_intersection orders it.
  *
- * Techniques: IP merges, HI hashes and BITMAP bit-tests the two sets tile by
- * tile (value-pivot tiles of <= 6144 elements per set, both sets streamed
- * once); OBS searches every element of the smaller set in the larger one
+ * Techniques: IP merges and HI hashes the two sets tile by tile (value-pivot
+ * tiles of <= 6144 elements per set, both sets streamed once); BITMAP ANDs
+ * the two parts' bitmaps per tile (tiles of <= 16384 elements per set) and
+ * orders the output by a scan of the tile counts, through a scratch array as
+ * long as the smaller set (so its workspace is about 4 min(nA, nB) bytes
+ * larger); OBS searches every element of the smaller set in the larger one
  * (cached top levels in shared memory); AUTO takes OBS when one set is more
  * than 64 times larger than the other, else BITMAP.
  *
@@ -218,7 +221,8 @@ si_status si_misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, u
  * the launching stream while enabled -- the counterpart of the reference's
  * DeviceTimer (include/device_timer.cuh:20-78), which wraps every phase of
  * every executable the same way.  Phase names: single pair "sisi_prepare",
- * "sisi_split", "sisi_tile"; dense all pairs "mm_incidence", "mm_gemm",
+ * "sisi_split", "sisi_tile", and for BITMAP with elements "sisi_scan",
+ * "sisi_copy"; dense all pairs "mm_incidence", "mm_gemm",
  * "naive_bitmaps", "naive_popcount"; all pairs of a tile "misi_plan",
  * "misi_probe"; single pair by search "obs_sample", "obs_search", "obs_scan",
  * "obs_compact"; batched pairs "batch_plan", "batch_count".  si_timer_read synchronises on
