@@ -12,6 +12,9 @@ the reference's own CPU executables, compiled from the reference sources by
   <name>.elements.bin ref_elements <name>.bin ...   (std::set_intersection of sets 0 and 1 through the
                                                      reference's readDataset): u64 n + u32[n]
   text_sets_asc.bin / text_sets_desc.bin            txt2bin text_sets.txt text_sets (src/txt2bin.cpp)
+  degree_<name>.bin, degree_<name>_{degree_set,degree_element,set_cdf,element_cdf}.txt
+                                                    degree_cdf <bin> <prefix> (src/degree_cdf.cpp) on
+                                                    datasets whose values stay below the universe
   text_roundtrip.txt                                bin2txt text_sets_asc.bin text_roundtrip (src/bin2txt.cpp)
 
 Run from the repository root in a container that has the reference checkout:
@@ -74,6 +77,27 @@ def datasets():
     return out
 
 
+def degree_datasets():
+    """Inputs of degree_cdf: values below the universe (the reference's inverted
+    index has `universe` slots), many equal set sizes and equal inverted-list
+    lengths (ties keep std::sort's order), empty sets."""
+    rng = np.random.default_rng(314159)
+    out = {}
+    U = 2048
+    sets = [np.zeros(0, np.uint32)]
+    for n in rng.integers(0, 6, size=30) * 25:  # sizes 0, 25, ..., 125: many ties
+        sets.append(uniq_sorted(rng, int(n), 0, U - 1))
+    out["degree_ties"] = fmt.from_sets(sets, universe=U)
+    # popular low values: skewed inverted-list lengths
+    V = 5000
+    p = 1.0 / np.arange(1, V) ** 0.9
+    p /= p.sum()
+    sets = [np.unique(rng.choice(np.arange(1, V), size=int(n), p=p)).astype(np.uint32)
+            for n in rng.integers(1, 600, size=60)]
+    out["degree_zipf"] = fmt.from_sets(sets, universe=V)
+    return out
+
+
 def run(cmd, cwd=None):
     r = subprocess.run(cmd, capture_output=True, text=True, cwd=cwd)
     if r.returncode != 0:
@@ -86,7 +110,8 @@ def sha(path):
 
 
 def main():
-    for exe in ("stdintersection", "serial_intersect", "boost_bitset", "ref_elements", "txt2bin", "bin2txt"):
+    for exe in ("stdintersection", "serial_intersect", "boost_bitset", "ref_elements", "txt2bin", "bin2txt",
+                "degree_cdf"):
         if not os.access(os.path.join(REF, exe), os.X_OK):
             raise SystemExit(f"oracle/_ref/{exe} missing: run `make -C oracle ref` first")
     manifest = {}
@@ -115,6 +140,14 @@ def main():
     run([os.path.join(REF, "bin2txt"), "text_sets_asc.bin", "text_roundtrip"], cwd=HERE)
     manifest["text_tools"] = {f: sha(os.path.join(HERE, f)) for f in
                               ("text_sets.txt", "text_sets_asc.bin", "text_sets_desc.bin", "text_roundtrip.txt")}
+    # dataset statistics
+    for name, ds in degree_datasets().items():
+        binp = os.path.join(HERE, f"{name}.bin")
+        fmt.write_dataset(binp, ds)
+        run([os.path.join(REF, "degree_cdf"), binp, name], cwd=HERE)
+        manifest[name] = {f: sha(os.path.join(HERE, f)) for f in
+                          [f"{name}.bin"] + [f"{name}_{t}.txt" for t in
+                                             ("degree_set", "degree_element", "set_cdf", "element_cdf")]}
     with open(os.path.join(HERE, "MANIFEST.json"), "w") as f:
         json.dump(manifest, f, indent=1, sort_keys=True)
     print(json.dumps({k: len(v) for k, v in manifest.items()}))
