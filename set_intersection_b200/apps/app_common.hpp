@@ -11,6 +11,12 @@
 // --buckets, --bucket-size) are accepted and ignored: the engine sizes its own
 // launches for the GPU it runs on.
 //
+// --output-binary <path> (an addition) also writes every count as binary:
+// u32 k, u32 0, u64 C(k, 2), then the u32 counts of pairs (i, j), i < j, in
+// row order (0,1), (0,2), ..., (0,k-1), (1,2), ... -- the triangular index of
+// include/util.hpp:68-70 -- for loading into numpy or another tool without
+// parsing text.
+//
 // Exit status: 0 on success, 1 on a flag or input error (as the reference),
 // 2 on a device or library error (the reference exits with the CUDA error
 // code, include/helpers.cuh:63-72).
@@ -94,7 +100,7 @@ inline std::vector<std::pair<Tile, Tile>> tile_pairs(uint32_t k, uint32_t partit
 inline uint64_t tri(uint64_t n, uint64_t i, uint64_t j) { return n * (n - 1) / 2 - (n - i) * (n - i - 1) / 2 + j - i - 1; }
 
 struct Args {
-    std::string input, output;
+    std::string input, output, output_binary;
     uint32_t partition = 10000;
     bool help = false;
 };
@@ -137,6 +143,8 @@ inline bool parse_args(int argc, char** argv, const std::set<std::string>& value
             a.input = val;
         } else if (s == "output") {
             a.output = val;
+        } else if (s == "output-binary") {
+            a.output_binary = val;
         } else {
             char* end = nullptr;
             const unsigned long v = std::strtoul(val.c_str(), &end, 10);
@@ -269,12 +277,14 @@ inline int run(const Spec& spec, int argc, char** argv) {
     std::set<std::string> vflags = spec.value_flags;
     vflags.insert("input");
     vflags.insert("output");
+    vflags.insert("output-binary");
     if (!parse_args(argc, argv, vflags, spec.bool_flags, a, why)) {
         std::printf("%s\n", why.c_str());
         return 1;
     }
     if (a.help) {
-        std::printf("%s\nUsage: %s --input <dataset> [--output <result>]", spec.banner, spec.name);
+        std::printf("%s\nUsage: %s --input <dataset> [--output <result>] [--output-binary <counts.bin>]", spec.banner,
+                    spec.name);
         for (auto& f : spec.value_flags) std::printf(" [--%s <n>]", f.c_str());
         for (auto& f : spec.bool_flags) std::printf(" [--%s]", f.c_str());
         std::printf("\n");
@@ -397,6 +407,13 @@ inline int run(const Spec& spec, int argc, char** argv) {
             auto r1 = std::chrono::steady_clock::now();
             SI_APP_CUDA(cudaMemcpy(rc[cur].data(), d_counts, run_counts * 4, cudaMemcpyDeviceToHost));
             auto r2 = std::chrono::steady_clock::now();
+            if (!a.output_binary.empty()) {  // into the whole-collection triangle
+                const bool self = A.id == B.id;
+                for (uint32_t i = A.start; i < A.end; ++i)
+                    for (uint32_t j = self ? i + 1 : B.start; j < B.end; ++j)
+                        counts[tri(k, i, j)] = rc[cur][self ? tri(stride, i - A.start, j - A.start)
+                                                            : uint64_t(i - A.start) * stride + (j - B.start)];
+            }
             if (!a.output.empty()) {
                 out.run_async(A, B, rc[cur].data(), stride);  // waits for the run before the previous one
                 cur ^= 1;
@@ -428,6 +445,17 @@ inline int run(const Spec& spec, int argc, char** argv) {
     rows.push_back({"Total", buf});
     box("────────────────Timings (in ms)────────────────────", rows);
 
+    if (!a.output_binary.empty()) {
+        FILE* f = std::fopen(a.output_binary.c_str(), "wb");
+        const uint32_t zero = 0;
+        bool ok = f && std::fwrite(&k, 4, 1, f) == 1 && std::fwrite(&zero, 4, 1, f) == 1 &&
+                  std::fwrite(&pairs, 8, 1, f) == 1 && std::fwrite(counts.data(), 4, pairs, f) == pairs;
+        if (f) ok = std::fclose(f) == 0 && ok;
+        if (!ok) {
+            std::printf("cannot write %s\n", a.output_binary.c_str());
+            return 1;
+        }
+    }
     if (!a.output.empty()) {
         // the whole-collection counts (single pair, dense path) follow the
         // runs' order: a run is a self tile or a cross tile of the triangle

@@ -208,3 +208,21 @@ def test_generate_dataset_flag_errors(apps, tmp_path, args, msg):
     r = run("generate_dataset", "--output", str(tmp_path / "g"), *args)
     assert r.returncode == 1 and msg in r.stdout
     assert run("generate_dataset", "--help").returncode == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("app", ["ip", "bitmap_dynamic", "matrix_multiplication"])
+@pytest.mark.parametrize("partition", [7, 10000])
+def test_binary_counts_dump(cuda, apps, tmp_path, app, partition):
+    """--output-binary: u32 k, u32 0, u64 C(k,2), u32 counts in triangular order,
+    equal to the reference's result file (streamed runs and whole-triangle paths)."""
+    ds = fmt.read_dataset(golden_path("misi_mixed.bin"))
+    want = fmt.parse_result(golden_path("misi_mixed.std.txt"), ds.cardinality)
+    dump = tmp_path / "counts.bin"
+    r = run(app, "--input", golden_path("misi_mixed.bin"), "--output-binary", str(dump), "--partition", str(partition))
+    assert r.returncode == 0, r.stdout + r.stderr
+    raw = dump.read_bytes()
+    k, zero = np.frombuffer(raw[:8], dtype=np.uint32)
+    pairs = np.frombuffer(raw[8:16], dtype=np.uint64)[0]
+    assert (k, zero, pairs) == (ds.cardinality, 0, want.size)
+    assert np.array_equal(np.frombuffer(raw[16:], dtype=np.uint32).astype(np.uint64), want)
