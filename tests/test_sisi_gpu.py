@@ -176,17 +176,37 @@ def test_full_size_2_28(cuda, tech):
 
 
 @pytest.mark.parametrize("tech", TECHS)
-@pytest.mark.parametrize("gap", [1, 2, 8, 30, 31, 33, 64, 1 << 12, 1 << 20])
+@pytest.mark.parametrize("gap", [1, 2, 8, 15, 16, 17, 30, 31, 33, 64, 1 << 12, 1 << 20])
 def test_value_span_per_tile(cuda, tech, gap):
     """Tiles whose value span is below, at and above the bitmap capacity
-    (65536 values): the bitmap technique must fall back to the merge path
-    exactly where its bitmap cannot hold the span."""
+    (131072 values for the bitmap engine's tiles of about 8192 elements per
+    set: gaps near 16): tiles the bitmaps cannot hold take the search path."""
     rng = np.random.default_rng(gap)
     n = 60000
     hi = min(n * gap * 2, 1 << 32)
     a = _u(rng, n, hi)
     b = np.unique(np.concatenate([_u(rng, n, hi), a[::3]])).astype(np.uint32)
     check(a, b, tech)
+
+
+@pytest.mark.parametrize("tech", TECHS)
+def test_density_changes_within_one_pair(cuda, tech):
+    """One call mixes tiles that fit the bitmaps with tiles that do not: a dense
+    block, a sparse stretch, a second dense block and a sparse tail up to
+    2^32 - 1, with overlap in every region."""
+    rng = np.random.default_rng(99)
+    parts_a, parts_b = [], []
+    for lo, hi, n in ((0, 1 << 18, 100000), (1 << 18, 1 << 28, 40000), (1 << 28, (1 << 28) + (1 << 17), 60000),
+                      ((1 << 28) + (1 << 17), 1 << 32, 30000)):
+        a = lo + _u(rng, n, hi - lo).astype(np.int64)
+        b = lo + _u(rng, n, hi - lo).astype(np.int64)
+        b = np.union1d(b, a[::5])
+        parts_a.append(a)
+        parts_b.append(b)
+    a = np.unique(np.concatenate(parts_a)).astype(np.uint32)
+    b = np.unique(np.concatenate(parts_b)).astype(np.uint32)
+    check(a, b, tech)
+    check(b[::2].copy(), a, tech)
 
 
 def test_validate_sorted(cuda):
