@@ -108,7 +108,7 @@ def intersect(a: torch.Tensor, b: torch.Tensor, tech="ip", materialize: bool = T
 
 
 class HostPair:
-    """Device buffers and workspace reused by intersect_host across calls."""
+    """Device buffers, workspace and copy streams reused by intersect_host."""
 
     def __init__(self, device=None):
         self.device = torch.device(device if device is not None else "cuda")
@@ -116,41 +116,105 @@ class HostPair:
         self.dev_a = self.dev_b = self.dev_out = None
         self.count = torch.zeros(1, dtype=torch.int64, device=self.device)
         self.count_host = torch.zeros(1, dtype=torch.int64).pin_memory()
+        self.h2d = torch.cuda.Stream(self.device)
+        self.d2h = torch.cuda.Stream(self.device)
 
     def _fit(self, buf, n):
         if buf is None or buf.numel() < n:
             buf = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
         return buf
 
+    def _counts(self, n):
+        if self.count.numel() < n:
+            self.count = torch.zeros(n, dtype=torch.int64, device=self.device)
+            self.count_host = torch.zeros(n, dtype=torch.int64).pin_memory()
+
+
+def _split_points(a, b, chunks: int):
+    """Chunk bounds of two sorted host sets at common value pivots: chunk i
+    holds the values in [v_i, v_(i+1)) of both sets, so the intersection is the
+    concatenation of the chunks' intersections.  The pivots are evenly spaced
+    elements of the larger set; the smaller set is cut where they fall."""
+    import numpy as np
+    big, small = (a, b) if a.size >= b.size else (b, a)
+    ib = np.array([big.size * i // chunks for i in range(chunks + 1)], dtype=np.int64)
+    iS = np.concatenate([[0], np.searchsorted(small, big[ib[1:-1]], side="left"), [small.size]]).astype(np.int64)
+    return (ib, iS) if a.size >= b.size else (iS, ib)
+
 
 def intersect_host(a_host: torch.Tensor, b_host: torch.Tensor, tech="ip", out_host: torch.Tensor | None = None,
-                   ctx: HostPair | None = None, stream=None):
+                   ctx: HostPair | None = None, stream=None, chunks: int | None = None):
     """End-to-end single pair from HOST sets: copies a and b to the device,
     intersects, and copies the count and the sorted elements back.
 
     a_host/b_host: 1-D int32/uint32 CPU tensors (pinned for asynchronous
     copies).  out_host: optional pinned int32 buffer of >= min(|a|, |b|)
-    elements that receives the result.  Returns (count, host tensor view)."""
+    elements that receives the result (allocated when None).  Returns
+    (count, host tensor view).
+
+    The pair is cut into `chunks` value ranges (default 8 for pairs of 2^22
+    elements or more, else 1) that are pipelined: chunk i's sets go to the
+    device on one copy stream while chunk i - 1 is intersected on `stream` and
+    the elements of earlier chunks come back on a second copy stream, so the
+    call takes about as long as the host-to-device copy of the inputs."""
+    import numpy as np
     ctx = ctx or HostPair()
     s = stream if stream is not None else torch.cuda.current_stream()
     n_a, n_b = a_host.numel(), b_host.numel()
+    n_min = min(n_a, n_b)
+    if out_host is None:
+        out_host = torch.empty(max(n_min, 1), dtype=torch.int32).pin_memory()
+    if n_min == 0:
+        return 0, out_host[:0]
+    if chunks is None:
+        chunks = 8 if n_a + n_b >= (1 << 22) else 1
+    C = max(1, min(int(chunks), n_min))
+    a_np = a_host.numpy().view(np.uint32)
+    b_np = b_host.numpy().view(np.uint32)
+    ia, ib = _split_points(a_np, b_np, C)
+    na = np.diff(ia)
+    nb = np.diff(ib)
+    cap = np.minimum(na, nb)
+    o_dev = np.concatenate([[0], np.cumsum(cap)]).astype(np.int64)  # chunk i's device output region
     ctx.dev_a = ctx._fit(ctx.dev_a, n_a)
     ctx.dev_b = ctx._fit(ctx.dev_b, n_b)
-    ctx.dev_out = ctx._fit(ctx.dev_out, min(n_a, n_b))
-    da, db = ctx.dev_a[:n_a], ctx.dev_b[:n_b]
+    ctx.dev_out = ctx._fit(ctx.dev_out, n_min)
+    ctx._counts(C)
+    ws_need = max(sisi_workspace_size(int(x), int(y), tech) for x, y in zip(na, nb))
     with torch.cuda.stream(s):
-        da.copy_(a_host.view(torch.int32), non_blocking=True)
-        db.copy_(b_host.view(torch.int32), non_blocking=True)
-        sisi_into(da, db, ctx.count, ctx.dev_out, ctx.ws, tech, s)
-        ctx.count_host.copy_(ctx.count, non_blocking=True)
-    s.synchronize()
-    c = int(ctx.count_host[0])
-    if out_host is None:
-        out_host = torch.empty(max(c, 1), dtype=torch.int32).pin_memory()
-    with torch.cuda.stream(s):
-        out_host[:c].copy_(ctx.dev_out[:c], non_blocking=True)
-    s.synchronize()
-    return c, out_host[:c]
+        ctx.ws.get(ws_need)  # sized before the pipeline starts
+    ai = a_host.view(torch.int32)
+    bi = b_host.view(torch.int32)
+    ev_in = [torch.cuda.Event() for _ in range(C)]
+    ev_out = [torch.cuda.Event() for _ in range(C)]
+    ctx.h2d.wait_stream(s)
+    for i in range(C):
+        a0, a1, b0, b1 = int(ia[i]), int(ia[i + 1]), int(ib[i]), int(ib[i + 1])
+        with torch.cuda.stream(ctx.h2d):
+            ctx.dev_a[a0:a1].copy_(ai[a0:a1], non_blocking=True)
+            ctx.dev_b[b0:b1].copy_(bi[b0:b1], non_blocking=True)
+            ev_in[i].record(ctx.h2d)
+    for i in range(C):
+        a0, a1, b0, b1 = int(ia[i]), int(ia[i + 1]), int(ib[i]), int(ib[i + 1])
+        s.wait_event(ev_in[i])
+        out_i = ctx.dev_out[int(o_dev[i]):int(o_dev[i + 1])] if cap[i] > 0 else None
+        sisi_into(ctx.dev_a[a0:a1], ctx.dev_b[b0:b1], ctx.count[i:i + 1], out_i, ctx.ws, tech, s)
+        with torch.cuda.stream(s):
+            ctx.count_host[i:i + 1].copy_(ctx.count[i:i + 1], non_blocking=True)
+            ev_out[i].record(s)
+    total = 0
+    for i in range(C):
+        ev_out[i].synchronize()
+        c = int(ctx.count_host[i])
+        if c:
+            ctx.d2h.wait_event(ev_out[i])
+            with torch.cuda.stream(ctx.d2h):
+                src = ctx.dev_out[int(o_dev[i]):int(o_dev[i]) + c]
+                out_host[total:total + c].copy_(src, non_blocking=True)
+        total += c
+    ctx.d2h.synchronize()
+    s.wait_stream(ctx.d2h)
+    return total, out_host[:total]
 
 
 class Collection:

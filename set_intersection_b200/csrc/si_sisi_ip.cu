@@ -717,7 +717,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
 //       clears them: one barrier of the 31 warps per tile (two with element
 //       output, for the block scan).
 //  K4b  exclusive scan of the tile counts (CUB), total into d_count.
-//  K5b  bm_copy_kernel: every tile's hits from scratch to their offset.
+//  K5b  bm_copy_kernel: every tile's hits from scratch to their offset (a warp per tile).
 // Count-only mode runs K3b alone and adds the hits into d_count.
 // Extra traffic over the algorithmic bytes: the matches written and read once
 // more through the scratch array.
@@ -1006,35 +1006,55 @@ __global__ void __launch_bounds__(kBmBlock, 1) bm_stage_kernel(
 }
 
 // K5b: tile t's tile_count[t] hits at scratch[split_y[t] ...] go to
-// out[tile_offset[t] ...].  One block per tile, grid-stride.
-constexpr int kBmCopyUnroll = 4;
+// out[tile_offset[t] ...].  One warp per tile, grid-stride over the tiles; the
+// next tile's count and offsets are loaded while the current one is copied,
+// and each lane keeps 8 loads in flight.
+constexpr int kBmCopyUnroll = 8;
 __global__ void __launch_bounds__(256) bm_copy_kernel(const uint32_t* __restrict__ tile_count,
                                                       const uint64_t* __restrict__ tile_offset,
                                                       const uint64_t* __restrict__ split_y, uint64_t nTiles,
                                                       const uint32_t* __restrict__ scratch, uint32_t* __restrict__ out,
                                                       uint64_t out_cap, uint32_t* err) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x / 32);
+    uint64_t t = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
     bool overflow = false;
-    for (uint64_t t = blockIdx.x; t < nTiles; t += gridDim.x) {
-        const uint32_t n = tile_count[t];
-        if (n == 0) continue;  // block-uniform
-        const uint32_t* src = scratch + split_y[t];
-        const uint64_t o = tile_offset[t];
-        for (uint32_t i0 = 0; i0 < n; i0 += blockDim.x * kBmCopyUnroll) {
+    uint32_t n = 0;
+    uint64_t o = 0, src = 0;
+    if (t < nTiles) {
+        n = tile_count[t];
+        o = tile_offset[t];
+        src = split_y[t];
+    }
+    while (t < nTiles) {  // warp-uniform
+        const uint64_t tn = t + warps;
+        uint32_t n2 = 0;
+        uint64_t o2 = 0, src2 = 0;
+        if (tn < nTiles) {
+            n2 = tile_count[tn];
+            o2 = tile_offset[tn];
+            src2 = split_y[tn];
+        }
+        for (uint32_t i0 = 0; i0 < n; i0 += 32 * kBmCopyUnroll) {
             uint32_t v[kBmCopyUnroll];
 #pragma unroll
             for (int u = 0; u < kBmCopyUnroll; ++u) {
-                const uint32_t i = i0 + u * blockDim.x + threadIdx.x;
-                v[u] = i < n ? __ldg(src + i) : 0u;
+                const uint32_t i = i0 + 32 * u + lane;
+                v[u] = i < n ? __ldg(scratch + src + i) : 0u;
             }
 #pragma unroll
             for (int u = 0; u < kBmCopyUnroll; ++u) {
-                const uint32_t i = i0 + u * blockDim.x + threadIdx.x;
+                const uint32_t i = i0 + 32 * u + lane;
                 if (i < n) {
                     if (o + i < out_cap) out[o + i] = v[u];
                     else overflow = true;
                 }
             }
         }
+        t = tn;
+        n = n2;
+        o = o2;
+        src = src2;
     }
     if (overflow) record_error(err, SI_ERR_OUTPUT_OVERFLOW, 9, 0);
 }
@@ -1155,8 +1175,8 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
         }
         {
             PhaseTimer timer("sisi_copy", stream);
-            const unsigned grid =
-                static_cast<unsigned>(std::min<uint64_t>(L.nTiles, static_cast<uint64_t>(sm_count()) * 8));
+            const unsigned grid = static_cast<unsigned>(
+                std::min<uint64_t>((L.nTiles + 7) / 8, static_cast<uint64_t>(sm_count()) * 8));
             bm_copy_kernel<<<std::max(grid, 1u), 256, 0, stream>>>(tile_count, tile_offset, split_y, L.nTiles, scratch,
                                                                    d_out, out_cap, reinterpret_cast<uint32_t*>(w));
             SI_LAUNCH_CHECK("bm_copy_kernel");

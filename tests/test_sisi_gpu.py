@@ -216,3 +216,28 @@ def test_validate_sorted(cuda):
     x[54321] = x[54320]
     assert not api.validate_sorted(dev(x))
     assert api.validate_sorted(dev(np.zeros(1, np.uint32)))
+
+
+@pytest.mark.parametrize("chunks", [None, 1, 3, 8])
+@pytest.mark.parametrize("tech", ["auto", "ip", "bitmap"])
+def test_intersect_host_pipeline(cuda, tech, chunks):
+    """The host-buffer call, cut into value-range chunks that are copied,
+    intersected and copied back in a pipeline: the same count and elements as
+    the oracle for balanced, skewed, tiny, empty and identical pairs."""
+    import torch
+    from set_intersection_b200 import api
+    rng = np.random.default_rng(5)
+    big = _u(rng, 1 << 21, 1 << 26)
+    cases = [(big, _u(rng, 1 << 21, 1 << 26)),                     # balanced, >= 2^22 elements: 8 chunks by default
+             (_u(rng, 3000, 1 << 26), big),                        # skewed
+             (np.array([5, 9], np.uint32), np.array([1, 5, 7, 9, 11], np.uint32)),  # fewer elements than chunks
+             (np.zeros(0, np.uint32), big[:100].copy()),           # one empty
+             (big[:500000].copy(), big[:500000].copy())]           # identical
+    ctx = api.HostPair()
+    for a, b in cases:
+        want = oracle.set_intersection(a, b)
+        ha = torch.from_numpy(a.view(np.int32)).pin_memory()
+        hb = torch.from_numpy(b.view(np.int32)).pin_memory()
+        c, got = api.intersect_host(ha, hb, tech, ctx=ctx, chunks=chunks)
+        assert c == want.size
+        assert np.array_equal(got.numpy().view(np.uint32), want)
