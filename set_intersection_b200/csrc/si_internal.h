@@ -45,8 +45,9 @@ private:
 };
 
 // ---- single-pair tile pipeline (si_sisi_ip.cu) ----
-// inner: 0 = merge path (technique ip), 1 = bitmap probe (technique bitmap),
-// 2 = hash probe (technique hi).
+// inner: 0 = merge path (technique ip), 1 = the bitmap engine (technique
+// bitmap: two bitmaps per tile AND-ed, bm_stage_kernel), 2 = hash probe
+// (technique hi).  The bitmap engine's workspace is larger (its scratch array).
 size_t ip_workspace_size(uint64_t nA, uint64_t nB, int inner = 0);
 // SI_TECH_AUTO searches the smaller set in the larger (obs) when the sizes
 // differ by more than this factor.
