@@ -697,16 +697,15 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// Technique bitmap: three launches after the pivot split, with no ordering
+// Technique bitmap: three steps after the pivot split, with no ordering
 // between tiles (no look-back).
 //
 //  K3b  bm_stage_kernel, persistent, one CTA of 32 warps per SM.  Warp 31
 //       stages tiles (ticket order) into a shared-memory ring with bulk
 //       copies, several tiles ahead; warps 0-30 take them in turn.  Both parts
 //       of a tile become bitmaps of the value range they share, [lo, hi] =
-//       [max of the firsts, min of the lasts] (16-byte shared loads, the bits
-//       of one thread's four values OR-ed per word in a register, one shared
-//       atomic OR per word); the AND of the two bitmaps is the tile's
+//       [max of the firsts, min of the lasts] (16-byte shared loads, one
+//       predicated shared atomic OR per value); the AND of the two bitmaps is the tile's
 //       intersection, already in value order.  Each thread takes a run of
 //       words, counts its bits; a block scan places the runs and the threads
 //       write lo + bit index of every set bit to scratch[tile's first Y
