@@ -92,6 +92,28 @@ si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
                   si_technique t, uint64_t* d_count, uint32_t* d_out, uint64_t out_cap,
                   void* d_workspace, size_t workspace_bytes, si_stream_t stream);
 
+/* Single pair from HOST buffers: copies A and B to the device, intersects
+ * them and copies the count and (when h_out is non-NULL) the sorted elements
+ * back; returns when *count and h_out are final.  The path of the reference's
+ * executables for a 2-set file (src/ip.cu:129-177: the dataset copied with
+ * cudaMemcpy, the kernels, the count copied back), as one call.
+ *
+ * The pair is cut into `chunks` value ranges (0: 8 for pairs of 2^22 elements
+ * or more, else 1; at most 64) that are pipelined: one range's sets are copied
+ * up while the previous range is intersected and the elements of earlier
+ * ranges are copied down, so with pinned host buffers the call costs about the
+ * host-to-device copy.  Pageable buffers work too, without the overlap.
+ *
+ * d_workspace: device, 256-byte aligned, of si_sisi_host_workspace_size bytes
+ * (it holds the device copies of both sets, the output and the per-range
+ * si_sisi workspace).  h_out: host uint32[out_cap], out_cap >= min(nA, nB).
+ * Technique t as in si_sisi (AUTO picks per range). */
+size_t si_sisi_host_workspace_size(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB,
+                                   si_technique t, uint32_t chunks);
+si_status si_sisi_host(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB, si_technique t,
+                       uint32_t chunks, uint64_t* count, uint32_t* h_out, uint64_t out_cap,
+                       void* d_workspace, size_t workspace_bytes, si_stream_t stream);
+
 /* Single pair without any caller-provided scratch.  No counterpart in the
  * reference (whose executables cudaMalloc everything themselves).
  *

@@ -108,113 +108,49 @@ def intersect(a: torch.Tensor, b: torch.Tensor, tech="ip", materialize: bool = T
 
 
 class HostPair:
-    """Device buffers, workspace and copy streams reused by intersect_host."""
+    """Device workspace reused by intersect_host across calls (it holds the
+    device copies of both sets, the output and the per-range scratch)."""
 
     def __init__(self, device=None):
         self.device = torch.device(device if device is not None else "cuda")
         self.ws = Workspace(self.device)
-        self.dev_a = self.dev_b = self.dev_out = None
-        self.count = torch.zeros(1, dtype=torch.int64, device=self.device)
-        self.count_host = torch.zeros(1, dtype=torch.int64).pin_memory()
-        self.h2d = torch.cuda.Stream(self.device)
-        self.d2h = torch.cuda.Stream(self.device)
-
-    def _fit(self, buf, n):
-        if buf is None or buf.numel() < n:
-            buf = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
-        return buf
-
-    def _counts(self, n):
-        if self.count.numel() < n:
-            self.count = torch.zeros(n, dtype=torch.int64, device=self.device)
-            self.count_host = torch.zeros(n, dtype=torch.int64).pin_memory()
 
 
-def _split_points(a, b, chunks: int):
-    """Chunk bounds of two sorted host sets at common value pivots: chunk i
-    holds the values in [v_i, v_(i+1)) of both sets, so the intersection is the
-    concatenation of the chunks' intersections.  The pivots are evenly spaced
-    elements of the larger set; the smaller set is cut where they fall."""
-    import numpy as np
-    big, small = (a, b) if a.size >= b.size else (b, a)
-    ib = np.array([big.size * i // chunks for i in range(chunks + 1)], dtype=np.int64)
-    iS = np.concatenate([[0], np.searchsorted(small, big[ib[1:-1]], side="left"), [small.size]]).astype(np.int64)
-    return (ib, iS) if a.size >= b.size else (iS, ib)
+def _check_host(x: torch.Tensor, name: str) -> None:
+    if x.dim() != 1 or x.is_cuda or not x.is_contiguous():
+        raise ValueError(f"{name} must be a 1-D contiguous CPU tensor")
+    if x.dtype not in (torch.int32, torch.uint32):
+        raise ValueError(f"{name} must hold uint32 bit patterns (int32 or uint32 dtype)")
 
 
 def intersect_host(a_host: torch.Tensor, b_host: torch.Tensor, tech="ip", out_host: torch.Tensor | None = None,
                    ctx: HostPair | None = None, stream=None, chunks: int | None = None):
-    """End-to-end single pair from HOST sets: copies a and b to the device,
-    intersects, and copies the count and the sorted elements back.
+    """End-to-end single pair from HOST sets through si_sisi_host: copies a and
+    b to the device, intersects, and copies the count and the sorted elements
+    back, pipelined over `chunks` value ranges (None: the library's default, 8
+    for pairs of 2^22 elements or more).
 
-    a_host/b_host: 1-D int32/uint32 CPU tensors (pinned for asynchronous
-    copies).  out_host: optional pinned int32 buffer of >= min(|a|, |b|)
-    elements that receives the result (allocated when None).  Returns
-    (count, host tensor view).
-
-    The pair is cut into `chunks` value ranges (default 8 for pairs of 2^22
-    elements or more, else 1) that are pipelined: chunk i's sets go to the
-    device on one copy stream while chunk i - 1 is intersected on `stream` and
-    the elements of earlier chunks come back on a second copy stream, so the
-    call takes about as long as the host-to-device copy of the inputs."""
-    import numpy as np
+    a_host/b_host: 1-D int32/uint32 CPU tensors (pinned, for the copies to
+    overlap).  out_host: optional int32 CPU buffer of >= min(|a|, |b|)
+    elements that receives the result (a pinned one is allocated when None).
+    Returns (count, host tensor view)."""
+    _check_host(a_host, "a_host")
+    _check_host(b_host, "b_host")
     ctx = ctx or HostPair()
     s = stream if stream is not None else torch.cuda.current_stream()
     n_a, n_b = a_host.numel(), b_host.numel()
-    n_min = min(n_a, n_b)
     if out_host is None:
-        out_host = torch.empty(max(n_min, 1), dtype=torch.int32).pin_memory()
-    if n_min == 0:
-        return 0, out_host[:0]
-    if chunks is None:
-        chunks = 8 if n_a + n_b >= (1 << 22) else 1
-    C = max(1, min(int(chunks), n_min))
-    a_np = a_host.numpy().view(np.uint32)
-    b_np = b_host.numpy().view(np.uint32)
-    ia, ib = _split_points(a_np, b_np, C)
-    na = np.diff(ia)
-    nb = np.diff(ib)
-    cap = np.minimum(na, nb)
-    o_dev = np.concatenate([[0], np.cumsum(cap)]).astype(np.int64)  # chunk i's device output region
-    ctx.dev_a = ctx._fit(ctx.dev_a, n_a)
-    ctx.dev_b = ctx._fit(ctx.dev_b, n_b)
-    ctx.dev_out = ctx._fit(ctx.dev_out, n_min)
-    ctx._counts(C)
-    ws_need = max(sisi_workspace_size(int(x), int(y), tech) for x, y in zip(na, nb))
-    with torch.cuda.stream(s):
-        ctx.ws.get(ws_need)  # sized before the pipeline starts
-    ai = a_host.view(torch.int32)
-    bi = b_host.view(torch.int32)
-    ev_in = [torch.cuda.Event() for _ in range(C)]
-    ev_out = [torch.cuda.Event() for _ in range(C)]
-    ctx.h2d.wait_stream(s)
-    for i in range(C):
-        a0, a1, b0, b1 = int(ia[i]), int(ia[i + 1]), int(ib[i]), int(ib[i + 1])
-        with torch.cuda.stream(ctx.h2d):
-            ctx.dev_a[a0:a1].copy_(ai[a0:a1], non_blocking=True)
-            ctx.dev_b[b0:b1].copy_(bi[b0:b1], non_blocking=True)
-            ev_in[i].record(ctx.h2d)
-    for i in range(C):
-        a0, a1, b0, b1 = int(ia[i]), int(ia[i + 1]), int(ib[i]), int(ib[i + 1])
-        s.wait_event(ev_in[i])
-        out_i = ctx.dev_out[int(o_dev[i]):int(o_dev[i + 1])] if cap[i] > 0 else None
-        sisi_into(ctx.dev_a[a0:a1], ctx.dev_b[b0:b1], ctx.count[i:i + 1], out_i, ctx.ws, tech, s)
-        with torch.cuda.stream(s):
-            ctx.count_host[i:i + 1].copy_(ctx.count[i:i + 1], non_blocking=True)
-            ev_out[i].record(s)
-    total = 0
-    for i in range(C):
-        ev_out[i].synchronize()
-        c = int(ctx.count_host[i])
-        if c:
-            ctx.d2h.wait_event(ev_out[i])
-            with torch.cuda.stream(ctx.d2h):
-                src = ctx.dev_out[int(o_dev[i]):int(o_dev[i]) + c]
-                out_host[total:total + c].copy_(src, non_blocking=True)
-        total += c
-    ctx.d2h.synchronize()
-    s.wait_stream(ctx.d2h)
-    return total, out_host[:total]
+        out_host = torch.empty(max(min(n_a, n_b), 1), dtype=torch.int32).pin_memory()
+    _check_host(out_host, "out_host")
+    t = int(technique(tech))
+    ch = int(chunks or 0)
+    need = lib.si_sisi_host_workspace_size(a_host.data_ptr(), n_a, b_host.data_ptr(), n_b, t, ch)
+    ws = ctx.ws.get(need)
+    count = ctypes.c_uint64(0)
+    st = lib.si_sisi_host(a_host.data_ptr(), n_a, b_host.data_ptr(), n_b, t, ch, ctypes.byref(count),
+                          out_host.data_ptr(), out_host.numel(), _ptr(ws), ws.numel(), _stream(s))
+    check(st, "si_sisi_host")
+    return int(count.value), out_host[:count.value]
 
 
 class Collection:

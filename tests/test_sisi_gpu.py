@@ -221,9 +221,10 @@ def test_validate_sorted(cuda):
 @pytest.mark.parametrize("chunks", [None, 1, 3, 8])
 @pytest.mark.parametrize("tech", ["auto", "ip", "bitmap"])
 def test_intersect_host_pipeline(cuda, tech, chunks):
-    """The host-buffer call, cut into value-range chunks that are copied,
-    intersected and copied back in a pipeline: the same count and elements as
-    the oracle for balanced, skewed, tiny, empty and identical pairs."""
+    """The host-buffer call (si_sisi_host), cut into value-range chunks that
+    are copied, intersected and copied back in a pipeline: the same count and
+    elements as the oracle for balanced, skewed, tiny, empty and identical
+    pairs, from pinned and from pageable host memory."""
     import torch
     from set_intersection_b200 import api
     rng = np.random.default_rng(5)
@@ -234,10 +235,12 @@ def test_intersect_host_pipeline(cuda, tech, chunks):
              (np.zeros(0, np.uint32), big[:100].copy()),           # one empty
              (big[:500000].copy(), big[:500000].copy())]           # identical
     ctx = api.HostPair()
-    for a, b in cases:
+    for n, (a, b) in enumerate(cases):
         want = oracle.set_intersection(a, b)
-        ha = torch.from_numpy(a.view(np.int32)).pin_memory()
-        hb = torch.from_numpy(b.view(np.int32)).pin_memory()
+        ha = torch.from_numpy(a.view(np.int32))
+        hb = torch.from_numpy(b.view(np.int32))
+        if n % 2 == 0:  # pinned (the copies overlap) and pageable buffers
+            ha, hb = ha.pin_memory(), hb.pin_memory()
         c, got = api.intersect_host(ha, hb, tech, ctx=ctx, chunks=chunks)
         assert c == want.size
         assert np.array_equal(got.numpy().view(np.uint32), want)
