@@ -20,8 +20,9 @@ Metric: Gelem/s = (|A| + |B|) / step time.
 
   value   device-timed (CUDA events on the launching stream), inputs resident
           in HBM; 2 GiB of input per step > 126 MB L2, so no L2 flush.
-  e2e     the same metric through the public host API (api.intersect_host):
-          pinned host sets -> H2D -> kernels -> count + elements D2H, per step.
+  e2e     the same metric through the host-buffer C-ABI call si_sisi_host
+          (via api.intersect_host): pinned host sets -> H2D -> kernels ->
+          count + elements D2H, per step, pipelined over 8 value ranges.
   roofline  live per-launch time of the dominant kernel (the tile kernel) from the
           library's phase timer over the timed region, against measured HBM;
           phase_avg_ms lists every phase of the step (split, tiles, scan, copy).
