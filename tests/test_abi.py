@@ -178,3 +178,36 @@ def test_skewed_generator_plants_overlap():
     assert a.size == 1 << 10 and b.size == 1 << 16
     assert np.all(b[1:] > b[:-1])
     assert oracle.count(a, b) >= int(round(0.2 * a.size))
+
+
+def test_host_pair_call_checks_arguments_on_host():
+    """si_sisi_host: argument errors and a too-small workspace come back before
+    any copy or launch; its workspace holds both sets, the output and the
+    per-range scratch, and grows with the input."""
+    L = si.lib
+    nul = ctypes.c_void_p(None)
+    fake = ctypes.c_void_p(0x10000)  # 256-byte aligned, never dereferenced
+    a = np.arange(0, 4000, 2, dtype=np.uint32)
+    b = np.arange(0, 3000, 3, dtype=np.uint32)
+    pa, pb = a.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p)
+    out = np.zeros(min(a.size, b.size), dtype=np.uint32)
+    po = out.ctypes.data_as(ctypes.c_void_p)
+    cnt = ctypes.c_uint64(7)
+    t = int(Technique.AUTO)
+    need = L.si_sisi_host_workspace_size(pa, a.size, pb, b.size, t, 4)
+    assert need >= 4 * (a.size + b.size + min(a.size, b.size))
+    assert L.si_sisi_host_workspace_size(pa, a.size << 1, pa, a.size << 1, t, 4) > 0
+    # null count, null workspace, misaligned workspace, short output, short workspace
+    assert L.si_sisi_host(pa, a.size, pb, b.size, t, 4, None, po, out.size, fake, need, nul) == Status.INVALID_ARGUMENT
+    assert L.si_sisi_host(pa, a.size, pb, b.size, t, 4, ctypes.byref(cnt), po, out.size, nul, need,
+                          nul) == Status.INVALID_ARGUMENT
+    assert L.si_sisi_host(pa, a.size, pb, b.size, t, 4, ctypes.byref(cnt), po, out.size, ctypes.c_void_p(0x10010),
+                          need, nul) == Status.INVALID_ARGUMENT
+    assert L.si_sisi_host(pa, a.size, pb, b.size, t, 4, ctypes.byref(cnt), po, out.size - 1, fake, need,
+                          nul) == Status.INVALID_ARGUMENT
+    assert L.si_sisi_host(pa, a.size, pb, b.size, t, 4, ctypes.byref(cnt), po, out.size, fake, need - 1,
+                          nul) == Status.WORKSPACE_TOO_SMALL
+    # an empty set: count 0 without touching the device
+    assert L.si_sisi_host(pa, 0, pb, b.size, t, 0, ctypes.byref(cnt), po, out.size, fake,
+                          L.si_sisi_host_workspace_size(pa, 0, pb, b.size, t, 0), nul) == Status.OK
+    assert cnt.value == 0
