@@ -272,17 +272,13 @@ def run_ours(args, rank: int, world: int):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        dist = dist_mod
-        dist.init_process_group("nccl", device_id=dev)
+    from set_intersection_b200.replicas import Replicas
+    rep = Replicas("nccl", dev)
 
     # inputs: rank 0 generates (or loads the cache), the others load the cache
     if rank == 0:
         a, b = make_pair(args.workload)
-    if dist:
-        dist.barrier()
+    rep.barrier()
     if rank != 0:
         a, b = make_pair(args.workload)
 
@@ -311,8 +307,7 @@ def run_ours(args, rank: int, world: int):
     for _ in range(args.warmup):
         step()
     stream.synchronize()
-    if dist:
-        dist.barrier()
+    rep.barrier()
     torch.cuda.synchronize()
 
     lib.si_timer_reset()
@@ -338,14 +333,11 @@ def run_ours(args, rank: int, world: int):
     lib.si_timer_reset()
     ws.check(stream)
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    rep.barrier()
+    ms_total = rep.max(ms_total)
 
     ms_step = ms_total / args.steps
-    value = world * (n_a + n_b) / (ms_step * 1e-3) / 1e9
+    value = rep.rate(n_a + n_b, ms_step) / 1e9
 
     # ---- end to end through the public host API ----
     e2e = None
@@ -357,8 +349,7 @@ def run_ours(args, rank: int, world: int):
         for _ in range(2):
             api.intersect_host(ha, hb, args.technique, hout, ctx, stream)
         e_steps = max(1, min(args.steps, args.e2e_steps))
-        if dist:
-            dist.barrier()
+        rep.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -367,19 +358,15 @@ def run_ours(args, rank: int, world: int):
         e1.record(stream)
         e1.synchronize()
         e_ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = rep.max(e_ms)
         e_step = e_ms / e_steps
-        e2e = {"value": world * (n_a + n_b) / (e_step * 1e-3) / 1e9, "unit": "Gelem/s",
+        e2e = {"value": rep.rate(n_a + n_b, e_step) / 1e9, "unit": "Gelem/s",
                "h2d_bytes_per_step": 4 * (n_a + n_b), "d2h_bytes_per_step": 8 + 4 * ce,
                "ms_per_step": e_step, "steps": e_steps}
         assert ce == c
 
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
+        rep.close()
         return
 
     # ---- roofline of the dominant kernel ----
@@ -438,8 +425,7 @@ def run_ours(args, rank: int, world: int):
     if world == 1 and not args.no_extras:
         line["other_workloads"] = other_workloads(args)
     print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
+    rep.close()
 
 
 # ------------------------------------------------------- MISI, dense form --
@@ -543,11 +529,8 @@ def run_ours_dense(args, rank: int, world: int):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        dist = dist_mod
-        dist.init_process_group("nccl", device_id=dev)
+    from set_intersection_b200.replicas import Replicas
+    rep = Replicas("nccl", dev)
     powerlaw = is_powerlaw(args.workload)
     if powerlaw:
         tech = args.technique if args.technique in ("ip", "obs", "hi", "bitmap", "auto") else "bitmap"
@@ -594,8 +577,7 @@ def run_ours_dense(args, rank: int, world: int):
     for _ in range(args.warmup):
         step()
     stream.synchronize()
-    if dist:
-        dist.barrier()
+    rep.barrier()
     torch.cuda.synchronize()
 
     gemm_phase = b"misi_probe" if powerlaw else b"mm_gemm" if tech == "mm" else b"naive_popcount"
@@ -615,13 +597,10 @@ def run_ours_dense(args, rank: int, world: int):
     lib.si_timer_reset()
     ws.check(stream)
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    rep.barrier()
+    ms_total = rep.max(ms_total)
     ms_step = ms_total / args.steps
-    value = world * pairs / (ms_step * 1e-3)
+    value = rep.rate(pairs, ms_step)
 
     # the plain AND-popcount kernel on the same GPU, for the speed-up
     plain_ms = None
@@ -648,8 +627,7 @@ def run_ours_dense(args, rank: int, world: int):
         else:
             api.misi_dense_host(h_el, h_off, universe, tech, dtype, h_counts, ctx, stream)
         e_steps = max(1, min(args.steps, args.e2e_steps))
-        if dist:
-            dist.barrier()
+        rep.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -661,18 +639,14 @@ def run_ours_dense(args, rank: int, world: int):
         e1.record(stream)
         e1.synchronize()
         e_ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = rep.max(e_ms)
         e_step = e_ms / e_steps
-        e2e = {"value": world * pairs / (e_step * 1e-3), "unit": "pairs/s",
+        e2e = {"value": rep.rate(pairs, e_step), "unit": "pairs/s",
                "h2d_bytes_per_step": int(4 * el.size + 8 * off.size), "d2h_bytes_per_step": int(4 * pairs),
                "ms_per_step": e_step, "steps": e_steps}
 
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
+        rep.close()
         return
 
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
@@ -737,8 +711,7 @@ def run_ours_dense(args, rank: int, world: int):
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def cublas_int8_tops(dev, n: int = 8192, reps: int = 10):
@@ -820,11 +793,8 @@ def run_ours_batch(args, rank: int, world: int):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        dist = dist_mod
-        dist.init_process_group("nccl", device_id=dev)
+    from set_intersection_b200.replicas import Replicas
+    rep = Replicas("nccl", dev)
     w = WORKLOADS[args.workload]
     el, off, pairs = batch_data(args.workload)
     k, npairs = off.size - 1, len(pairs)
@@ -853,8 +823,7 @@ def run_ours_batch(args, rank: int, world: int):
     for _ in range(args.warmup):
         graph.launch(stream)
     stream.synchronize()
-    if dist:
-        dist.barrier()
+    rep.barrier()
     torch.cuda.synchronize()
     lib.si_timer_reset()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -866,13 +835,10 @@ def run_ours_batch(args, rank: int, world: int):
         stop.synchronize()
     ms_total = start.elapsed_time(stop)
     graph.check(stream)
-    if dist:
-        dist.barrier()
-        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    rep.barrier()
+    ms_total = rep.max(ms_total)
     ms_step = ms_total / args.steps
-    value = world * npairs / (ms_step * 1e-3)
+    value = rep.rate(npairs, ms_step)
 
     # the batch kernel alone (phase timer on a direct call, outside the graph)
     lib.si_timer_enable(1)
@@ -918,8 +884,7 @@ def run_ours_batch(args, rank: int, world: int):
             stream.synchronize()
 
         e2e_step()
-        if dist:
-            dist.barrier()
+        rep.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -928,20 +893,16 @@ def run_ours_batch(args, rank: int, world: int):
         e1.record(stream)
         e1.synchronize()
         e_ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = rep.max(e_ms)
         e_step = e_ms / e_steps
-        e2e = {"value": world * npairs / (e_step * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": int(8 * npairs),
+        e2e = {"value": rep.rate(npairs, e_step), "unit": "pairs/s", "h2d_bytes_per_step": int(8 * npairs),
                "d2h_bytes_per_step": int(4 * npairs), "ms_per_step": e_step, "steps": e_steps,
                "note": "pool resident in HBM (the indexed collection); per step the query pairs go H2D and "
                        "the counts D2H through the graph"}
     graph.close()
 
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
+        rep.close()
         return
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
     sizes = np.diff(off)
@@ -980,8 +941,7 @@ def run_ours_batch(args, rank: int, world: int):
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
+    rep.close()
 
 
 # Short runs of the other configurations, for the record of a default run.
