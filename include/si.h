@@ -114,6 +114,23 @@ si_status si_sisi_host(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint
                        uint32_t chunks, uint64_t* count, uint32_t* h_out, uint64_t out_cap,
                        void* d_workspace, size_t workspace_bytes, si_stream_t stream);
 
+/* The same call with its host-side resources made once: a si_host_ctx holds
+ * the two copy streams, the per-range events and the pinned words that each
+ * range's count and error word land in.  si_sisi_host creates and destroys one
+ * per call; a caller that intersects many pairs creates one
+ * (si_host_ctx_create, on the device that is current then) and passes it to
+ * every si_sisi_host_ctx call on that device, which then creates, allocates
+ * and frees nothing.  Calls sharing a context must not overlap (one host
+ * thread at a time).  Errors recorded on the device by any range are reported
+ * (the first one); a set that descends across a range boundary is reported as
+ * SI_ERR_INVALID_INPUT before anything is launched. */
+typedef struct si_host_ctx si_host_ctx;
+si_status si_host_ctx_create(si_host_ctx** out);
+void si_host_ctx_destroy(si_host_ctx* ctx);
+si_status si_sisi_host_ctx(si_host_ctx* ctx, const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB,
+                           si_technique t, uint32_t chunks, uint64_t* count, uint32_t* h_out, uint64_t out_cap,
+                           void* d_workspace, size_t workspace_bytes, si_stream_t stream);
+
 /* Single pair without any caller-provided scratch.  No counterpart in the
  * reference (whose executables cudaMalloc everything themselves).
  *

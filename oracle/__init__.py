@@ -56,6 +56,8 @@ def lib() -> ctypes.CDLL:
         L.si_oracle_triangular_index.argtypes = [u64, u64, u64]
         L.si_oracle_is_strictly_increasing.restype = i
         L.si_oracle_is_strictly_increasing.argtypes = [vp, u64]
+        L.si_oracle_gen_uniform.restype = i
+        L.si_oracle_gen_uniform.argtypes = [u64, u64, u64, u64, vp]
         _lib = L
     return _lib
 
@@ -103,6 +105,30 @@ def pairs(elements, offsets, k: int, pair_list, threads: int = 0) -> np.ndarray:
     if rc != 0:
         raise RuntimeError("si_oracle_pairs failed")
     return out[: pl.size // 2]
+
+
+def gen_uniform(seed: int, n: int, hi: int, lo: int = 0) -> np.ndarray:
+    """The engine's seeded uniform n-subset of [lo, hi), ascending, restated in
+    C (si_oracle_gen_uniform), so a reference run reads the very sets the
+    engine is timed on without loading the engine's library."""
+    out = np.empty(max(n, 1), dtype=np.uint32)
+    rc = lib().si_oracle_gen_uniform(seed, n, lo, hi, _p(out))
+    if rc != 0:
+        raise RuntimeError(f"si_oracle_gen_uniform failed ({rc})")
+    return out[:n]
+
+
+def write_dataset(path: str, sets, universe: int) -> None:
+    """A dataset file in the reference's binary format (include/io.hpp:70-89:
+    u32 cardinality, u32 universe, u64 total elements, u32 sizes[], u32
+    elements[]), written with numpy only."""
+    sizes = np.array([len(x) for x in sets], dtype=np.uint32)
+    with open(path, "wb") as f:
+        np.array([len(sets), universe], dtype=np.uint32).tofile(f)
+        np.array([int(sizes.sum(dtype=np.uint64))], dtype=np.uint64).tofile(f)
+        sizes.tofile(f)
+        for x in sets:
+            np.ascontiguousarray(x, dtype=np.uint32).tofile(f)
 
 
 def is_strictly_increasing(x) -> bool:

@@ -17,6 +17,9 @@
  *   si_oracle_all_pairs         <- the OpenMP pair loops of src/std_set_intersection.cpp:58-76,
  *                                  src/serial_intersect.cpp:61-76, src/boost_bitset.cpp:60-84
  *   si_oracle_triangular_index  <- include/util.hpp:68-70
+ *   si_oracle_gen_uniform       <- no reference counterpart: the engine's seeded input
+ *                                  generator restated, so that the reference's executables
+ *                                  read the very sets the engine is timed on
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -176,4 +179,117 @@ int si_oracle_is_strictly_increasing(const uint32_t* x, uint64_t n)
     for (uint64_t i = 1; i < n; ++i)
         if (x[i - 1] >= x[i]) return 0;
     return 1;
+}
+
+/* ------------------------------------------------------------------------
+ * Seeded inputs for the reference's CPU executables.
+ *
+ * si_oracle_gen_uniform: the same n-subset of [lo, hi) as the engine's
+ * si_gen_uniform (so a reference run reads exactly the sets the engine was
+ * timed on, without loading the engine's library).  Restated from its
+ * definition:
+ *   dense (n > U/64, U = hi - lo): the n values v with the smallest keys
+ *     (hash32(seed, v) << 32 | (v - lo)), ascending; hash32 is the top half of
+ *     the splitmix64 finaliser of v + seed * 0x9e3779b97f4a7c15 + 0x632be59bd9b4e019;
+ *   sparse: the first n distinct values lo + floor(r * U / 2^64) of the
+ *     splitmix64 stream that starts at seed * 0x9e3779b97f4a7c15 + 0x2545f4914f6cdd1d,
+ *     sorted.
+ * tests/test_oracle.py checks it against si_gen_uniform on both branches. */
+static uint64_t gen_mix64(uint64_t x)
+{
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+static uint32_t gen_hash32(uint64_t seed, uint64_t v)
+{
+    return (uint32_t)(gen_mix64(v + seed * 0x9e3779b97f4a7c15ull + 0x632be59bd9b4e019ull) >> 32);
+}
+
+static int cmp_u32(const void* x, const void* y)
+{
+    uint32_t a = *(const uint32_t*)x, b = *(const uint32_t*)y;
+    return a < b ? -1 : a > b;
+}
+
+/* histogram of (hash >> 16), or of (hash & 0xffff) among hashes whose top half is bin1 */
+static void gen_hist(uint64_t seed, uint64_t lo, uint64_t U, int level, uint64_t bin1, uint64_t* hist)
+{
+#ifdef _OPENMP
+#pragma omp parallel
+#endif
+    {
+        uint64_t* h = calloc(65536, sizeof(uint64_t));
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+        for (int64_t v = 0; v < (int64_t)U; ++v) {
+            uint32_t x = gen_hash32(seed, lo + (uint64_t)v);
+            if (level == 0) ++h[x >> 16];
+            else if ((x >> 16) == bin1) ++h[x & 0xffff];
+        }
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+        for (int q = 0; q < 65536; ++q) hist[q] += h[q];
+        free(h);
+    }
+}
+
+int si_oracle_gen_uniform(uint64_t seed, uint64_t n, uint64_t lo, uint64_t hi, uint32_t* out)
+{
+    if (hi < lo || hi - lo > (1ull << 32) || n > hi - lo) return -1;
+    const uint64_t U = hi - lo;
+    if (n == 0) return 0;
+    if (n > U / 64) {
+        /* threshold t = the n-th smallest hash; values with hash < t are all
+         * taken, those with hash == t in increasing v until n are held */
+        uint64_t* hist = calloc(65536, sizeof(uint64_t));
+        if (!hist) return -2;
+        gen_hist(seed, lo, U, 0, 0, hist);
+        uint64_t need = n, bin1 = 0;
+        for (; bin1 < 65536; ++bin1) {
+            if (hist[bin1] >= need) break;
+            need -= hist[bin1];
+        }
+        memset(hist, 0, 65536 * sizeof(uint64_t));
+        gen_hist(seed, lo, U, 1, bin1, hist);
+        uint64_t bin2 = 0;
+        for (; bin2 < 65536; ++bin2) {
+            if (hist[bin2] >= need) break;
+            need -= hist[bin2];
+        }
+        free(hist);
+        const uint32_t thr = (uint32_t)((bin1 << 16) | bin2);
+        uint64_t p = 0, eq = 0;
+        for (uint64_t v = 0; v < U; ++v) {
+            uint32_t x = gen_hash32(seed, lo + v);
+            if (x < thr || (x == thr && eq++ < need)) out[p++] = (uint32_t)(lo + v);
+        }
+        return p == n ? 0 : -3;
+    }
+    /* sparse: open-addressing set of the values drawn so far */
+    uint64_t cap = 1;
+    while (cap < 4 * n) cap <<= 1;
+    uint64_t* table = calloc(cap, sizeof(uint64_t)); /* value + 1, 0 = empty */
+    if (!table) return -2;
+    uint64_t state = seed * 0x9e3779b97f4a7c15ull + 0x2545f4914f6cdd1dull, k = 0;
+    while (k < n) {
+        state += 0x9e3779b97f4a7c15ull;
+        const uint64_t r = gen_mix64(state);
+        const uint32_t v = (uint32_t)(lo + (uint64_t)(((unsigned __int128)r * U) >> 64));
+        uint64_t s = gen_mix64(v) & (cap - 1);
+        while (table[s] && table[s] != (uint64_t)v + 1) s = (s + 1) & (cap - 1);
+        if (!table[s]) {
+            table[s] = (uint64_t)v + 1;
+            out[k++] = v;
+        }
+    }
+    free(table);
+    qsort(out, n, sizeof(uint32_t), cmp_u32);
+    return 0;
 }

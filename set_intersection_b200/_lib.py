@@ -74,6 +74,10 @@ _SIGNATURES = {
     "si_sisi_host_workspace_size": (_sz, [_vp, _u64, _vp, _u64, _int, ctypes.c_uint32]),
     "si_sisi_host": (_int, [_vp, _u64, _vp, _u64, _int, ctypes.c_uint32, ctypes.POINTER(_u64), _vp, _u64, _vp, _sz,
                             _vp]),
+    "si_host_ctx_create": (_int, [ctypes.POINTER(_vp)]),
+    "si_host_ctx_destroy": (None, [_vp]),
+    "si_sisi_host_ctx": (_int, [_vp, _vp, _u64, _vp, _u64, _int, ctypes.c_uint32, ctypes.POINTER(_u64), _vp, _u64,
+                                _vp, _sz, _vp]),
     "si_workspace_check": (_int, [_vp, _vp]),
     "si_workspace_diagnostic": (_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     "si_validate_sorted": (_int, [_vp, _u64, _vp, _vp]),

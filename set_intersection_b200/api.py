@@ -108,12 +108,28 @@ def intersect(a: torch.Tensor, b: torch.Tensor, tech="ip", materialize: bool = T
 
 
 class HostPair:
-    """Device workspace reused by intersect_host across calls (it holds the
-    device copies of both sets, the output and the per-range scratch)."""
+    """What intersect_host reuses across calls: the device workspace (the
+    device copies of both sets, the output and the per-range scratch) and a
+    si_host_ctx (copy streams, per-range events, pinned count and error
+    words), so a call allocates nothing once the workspace has grown."""
 
     def __init__(self, device=None):
         self.device = torch.device(device if device is not None else "cuda")
         self.ws = Workspace(self.device)
+        self._ctx = ctypes.c_void_p(None)
+        with torch.cuda.device(self.device):
+            check(lib.si_host_ctx_create(ctypes.byref(self._ctx)), "si_host_ctx_create")
+
+    def close(self) -> None:
+        if self._ctx:
+            lib.si_host_ctx_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _check_host(x: torch.Tensor, name: str) -> None:
@@ -147,9 +163,11 @@ def intersect_host(a_host: torch.Tensor, b_host: torch.Tensor, tech="ip", out_ho
     need = lib.si_sisi_host_workspace_size(a_host.data_ptr(), n_a, b_host.data_ptr(), n_b, t, ch)
     ws = ctx.ws.get(need)
     count = ctypes.c_uint64(0)
-    st = lib.si_sisi_host(a_host.data_ptr(), n_a, b_host.data_ptr(), n_b, t, ch, ctypes.byref(count),
-                          out_host.data_ptr(), out_host.numel(), _ptr(ws), ws.numel(), _stream(s))
-    check(st, "si_sisi_host")
+    with torch.cuda.device(ctx.device):
+        st = lib.si_sisi_host_ctx(ctx._ctx, a_host.data_ptr(), n_a, b_host.data_ptr(), n_b, t, ch,
+                                  ctypes.byref(count), out_host.data_ptr(), out_host.numel(), _ptr(ws), ws.numel(),
+                                  _stream(s))
+    check(st, "si_sisi_host_ctx")
     return int(count.value), out_host[:count.value]
 
 

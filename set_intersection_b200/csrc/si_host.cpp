@@ -8,11 +8,17 @@
 // the concatenation of the ranges' intersections.  The ranges are pipelined
 // over three streams: range i's sets are copied up on one copy stream, range
 // i is intersected on the caller's stream once they have landed (si_sisi into
-// its own output region), its count comes back on the caller's stream, and as
-// soon as the host holds that count the range's elements are copied back on a
-// second copy stream to their final place in h_out.  The call therefore costs
-// about the host-to-device copy of the inputs (with pinned host buffers; from
-// pageable memory the copies are staged by the driver and do not overlap).
+// its own output region), its count and error word come back on the caller's
+// stream, and as soon as the host holds that count the range's elements are
+// copied back on a second copy stream to their final place in h_out.  The call
+// therefore costs about the host-to-device copy of the inputs (with pinned
+// host buffers; from pageable memory the copies are staged by the driver and
+// do not overlap).
+//
+// The copy streams, the per-range events and the pinned words the counts and
+// error words land in belong to a si_host_ctx, created once (si_host_ctx_create)
+// and reused by every si_sisi_host_ctx call; si_sisi_host creates and destroys
+// one per call.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,14 +28,25 @@
 #include "si.h"
 #include "si_internal.h"
 
+struct si_host_ctx {
+    static constexpr uint32_t kMaxChunks = 64;
+    int device = -1;
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t start = nullptr;
+    cudaEvent_t landed[kMaxChunks] = {}, counted[kMaxChunks] = {};
+    uint64_t* hcount = nullptr;  // pinned [kMaxChunks]
+    uint32_t* herr = nullptr;    // pinned [kMaxChunks][4]: each range's workspace error header
+};
+
 namespace si {
 namespace {
 
-constexpr uint32_t kMaxChunks = 64;
+constexpr uint32_t kMaxChunks = si_host_ctx::kMaxChunks;
 
 struct Chunks {
     uint32_t n = 0;
-    std::vector<uint64_t> a, b;  // n + 1 bounds each
+    std::vector<uint64_t> a, b;   // n + 1 bounds each
+    bool descent_at_cut = false;  // a set descends across a range boundary
 };
 
 Chunks split(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB, uint32_t chunks) {
@@ -50,6 +67,9 @@ Chunks split(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB, u
         const uint32_t v = big[ib[i]];
         is[i] = static_cast<uint64_t>(std::lower_bound(small, small + n_small, v) - small);
         is[i] = std::max(is[i], is[i - 1]);  // (monotone even for unsorted input)
+        // no range's kernels see the two elements either side of a cut
+        if (ib[i] > 0 && big[ib[i] - 1] >= big[ib[i]]) c.descent_at_cut = true;
+        if (is[i] > 0 && is[i] < n_small && small[is[i] - 1] >= small[is[i]]) c.descent_at_cut = true;
     }
     c.a = a_big ? ib : is;
     c.b = a_big ? is : ib;
@@ -76,24 +96,86 @@ Layout layout(const Chunks& c, uint64_t nA, uint64_t nB, si_technique t) {
     return L;
 }
 
-struct Streams {  // the copy streams, per-range events and pinned counts of one call
-    cudaStream_t up = nullptr, down = nullptr, caller = nullptr;
-    std::vector<cudaEvent_t> landed, counted;
-    uint64_t* hcount = nullptr;
-    ~Streams() {  // every copy of the call has finished before anything is freed, also on error paths
+// Host-side checks of a call, made before any CUDA call.  SI_OK with `done`
+// set means the result is final without a launch (an empty set).
+si_status host_args(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB, si_technique t,
+                    uint32_t chunks, uint64_t* count, uint32_t* h_out, uint64_t out_cap, void* d_workspace,
+                    size_t workspace_bytes, Chunks& c, Layout& L, bool& done) {
+    done = false;
+    if ((nA && !hA) || (nB && !hB) || !count || !d_workspace) return SI_ERR_INVALID_ARGUMENT;
+    if (h_out && out_cap < std::min(nA, nB)) return SI_ERR_INVALID_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(d_workspace) % 256 != 0) return SI_ERR_INVALID_ARGUMENT;
+    *count = 0;
+    c = split(hA, nA, hB, nB, chunks);
+    L = layout(c, nA, nB, t);
+    if (workspace_bytes < L.total) return SI_ERR_WORKSPACE_TOO_SMALL;
+    if (std::min(nA, nB) == 0) {
+        done = true;
+        return SI_OK;
+    }
+    if (c.descent_at_cut) return SI_ERR_INVALID_INPUT;
+    return SI_OK;
+}
+
+// Every copy of a call has finished before the call returns, on error paths
+// too (the caller may free or reuse its host buffers at once).
+struct Drain {
+    si_host_ctx* ctx;
+    cudaStream_t caller;
+    ~Drain() {
         cudaStreamSynchronize(caller);
-        if (up) cudaStreamSynchronize(up);
-        if (down) cudaStreamSynchronize(down);
-        for (auto e : landed) cudaEventDestroy(e);
-        for (auto e : counted) cudaEventDestroy(e);
-        if (up) cudaStreamDestroy(up);
-        if (down) cudaStreamDestroy(down);
-        if (hcount) cudaFreeHost(hcount);
+        cudaStreamSynchronize(ctx->up);
+        cudaStreamSynchronize(ctx->down);
     }
 };
 
 }  // namespace
 }  // namespace si
+
+extern "C" si_status si_host_ctx_create(si_host_ctx** out) {
+    if (!out) return SI_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    auto* c = new si_host_ctx;
+    auto fail = [&](cudaError_t e, const char* what) {
+        si_host_ctx_destroy(c);
+        return si::cuda_fail(e, what);
+    };
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e != cudaSuccess) return fail(e, "cudaGetDevice");
+    if ((e = cudaStreamCreateWithFlags(&c->up, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaStreamCreateWithFlags(&c->down, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaEventCreateWithFlags(&c->start, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    for (uint32_t i = 0; i < si::kMaxChunks; ++i) {
+        if ((e = cudaEventCreateWithFlags(&c->landed[i], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(e, "event");
+        if ((e = cudaEventCreateWithFlags(&c->counted[i], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(e, "event");
+    }
+    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&c->hcount), si::kMaxChunks * 8, cudaHostAllocDefault)) !=
+        cudaSuccess)
+        return fail(e, "cudaHostAlloc");
+    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&c->herr), si::kMaxChunks * 16, cudaHostAllocDefault)) !=
+        cudaSuccess)
+        return fail(e, "cudaHostAlloc");
+    *out = c;
+    return SI_OK;
+}
+
+extern "C" void si_host_ctx_destroy(si_host_ctx* c) {
+    if (!c) return;
+    if (c->up) cudaStreamSynchronize(c->up);
+    if (c->down) cudaStreamSynchronize(c->down);
+    for (uint32_t i = 0; i < si::kMaxChunks; ++i) {
+        if (c->landed[i]) cudaEventDestroy(c->landed[i]);
+        if (c->counted[i]) cudaEventDestroy(c->counted[i]);
+    }
+    if (c->start) cudaEventDestroy(c->start);
+    if (c->up) cudaStreamDestroy(c->up);
+    if (c->down) cudaStreamDestroy(c->down);
+    if (c->hcount) cudaFreeHost(c->hcount);
+    if (c->herr) cudaFreeHost(c->herr);
+    delete c;
+}
 
 extern "C" size_t si_sisi_host_workspace_size(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB,
                                               si_technique t, uint32_t chunks) {
@@ -102,17 +184,20 @@ extern "C" size_t si_sisi_host_workspace_size(const uint32_t* hA, uint64_t nA, c
     return si::layout(c, nA, nB, t).total;
 }
 
-extern "C" si_status si_sisi_host(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB, si_technique t,
-                                  uint32_t chunks, uint64_t* count, uint32_t* h_out, uint64_t out_cap,
-                                  void* d_workspace, size_t workspace_bytes, si_stream_t stream) {
-    if ((nA && !hA) || (nB && !hB) || !count || !d_workspace) return SI_ERR_INVALID_ARGUMENT;
-    if (h_out && out_cap < std::min(nA, nB)) return SI_ERR_INVALID_ARGUMENT;
-    if (reinterpret_cast<uintptr_t>(d_workspace) % 256 != 0) return SI_ERR_INVALID_ARGUMENT;
-    *count = 0;
-    const si::Chunks c = si::split(hA, nA, hB, nB, chunks);
-    const si::Layout L = si::layout(c, nA, nB, t);
-    if (workspace_bytes < L.total) return SI_ERR_WORKSPACE_TOO_SMALL;
-    if (std::min(nA, nB) == 0) return SI_OK;
+extern "C" si_status si_sisi_host_ctx(si_host_ctx* ctx, const uint32_t* hA, uint64_t nA, const uint32_t* hB,
+                                      uint64_t nB, si_technique t, uint32_t chunks, uint64_t* count, uint32_t* h_out,
+                                      uint64_t out_cap, void* d_workspace, size_t workspace_bytes,
+                                      si_stream_t stream) {
+    if (!ctx) return SI_ERR_INVALID_ARGUMENT;
+    si::Chunks c;
+    si::Layout L;
+    bool done = false;
+    const si_status arg = si::host_args(hA, nA, hB, nB, t, chunks, count, h_out, out_cap, d_workspace,
+                                        workspace_bytes, c, L, done);
+    if (arg != SI_OK || done) return arg;
+    int dev = -1;
+    SI_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != ctx->device) return SI_ERR_INVALID_ARGUMENT;  // the context's streams live on another device
     unsigned char* w = static_cast<unsigned char*>(d_workspace);
     uint32_t* dA = reinterpret_cast<uint32_t*>(w + L.off_a);
     uint32_t* dB = reinterpret_cast<uint32_t*>(w + L.off_b);
@@ -121,54 +206,44 @@ extern "C" si_status si_sisi_host(const uint32_t* hA, uint64_t nA, const uint32_
     void* ws = w + L.off_ws;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
 
-    si::Streams st;
-    st.caller = s;
-    SI_CUDA_TRY(cudaStreamCreateWithFlags(&st.up, cudaStreamNonBlocking));
-    SI_CUDA_TRY(cudaStreamCreateWithFlags(&st.down, cudaStreamNonBlocking));
-    st.landed.resize(c.n, nullptr);
-    st.counted.resize(c.n, nullptr);
-    for (uint32_t i = 0; i < c.n; ++i) {
-        SI_CUDA_TRY(cudaEventCreateWithFlags(&st.landed[i], cudaEventDisableTiming));
-        SI_CUDA_TRY(cudaEventCreateWithFlags(&st.counted[i], cudaEventDisableTiming));
-    }
+    si::Drain drain{ctx, s};
     // the copies up start after the caller's earlier work on its stream
-    cudaEvent_t start = nullptr;
-    SI_CUDA_TRY(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
-    st.landed.push_back(start);  // destroyed with the others
-    SI_CUDA_TRY(cudaEventRecord(start, s));
-    SI_CUDA_TRY(cudaStreamWaitEvent(st.up, start, 0));
+    SI_CUDA_TRY(cudaEventRecord(ctx->start, s));
+    SI_CUDA_TRY(cudaStreamWaitEvent(ctx->up, ctx->start, 0));
     for (uint32_t i = 0; i < c.n; ++i) {
         const uint64_t a0 = c.a[i], na = c.a[i + 1] - a0, b0 = c.b[i], nb = c.b[i + 1] - b0;
-        if (na) SI_CUDA_TRY(cudaMemcpyAsync(dA + a0, hA + a0, na * 4, cudaMemcpyHostToDevice, st.up));
-        if (nb) SI_CUDA_TRY(cudaMemcpyAsync(dB + b0, hB + b0, nb * 4, cudaMemcpyHostToDevice, st.up));
-        SI_CUDA_TRY(cudaEventRecord(st.landed[i], st.up));
+        if (na) SI_CUDA_TRY(cudaMemcpyAsync(dA + a0, hA + a0, na * 4, cudaMemcpyHostToDevice, ctx->up));
+        if (nb) SI_CUDA_TRY(cudaMemcpyAsync(dB + b0, hB + b0, nb * 4, cudaMemcpyHostToDevice, ctx->up));
+        SI_CUDA_TRY(cudaEventRecord(ctx->landed[i], ctx->up));
     }
     std::vector<uint64_t> out_at(c.n + 1, 0);  // each range's output region on the device
     for (uint32_t i = 0; i < c.n; ++i)
         out_at[i + 1] = out_at[i] + std::min(c.a[i + 1] - c.a[i], c.b[i + 1] - c.b[i]);
-    // the ranges' counts land in pinned memory, so waiting for one does not
-    // hold up the launches of the next
-    SI_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void**>(&st.hcount), size_t(c.n) * 8, cudaHostAllocDefault));
     uint64_t total = 0;
-    auto copy_down = [&](uint32_t i) -> si_status {  // range i's elements, once its count is known
-        SI_CUDA_TRY(cudaEventSynchronize(st.counted[i]));
-        const uint64_t ci = std::min(st.hcount[i], out_at[i + 1] - out_at[i]);
+    si_status first_error = SI_OK;
+    // range i's elements, once its count is known; and its error word: every
+    // range reuses the one workspace, whose header each range's kernels clear
+    auto copy_down = [&](uint32_t i) -> si_status {
+        SI_CUDA_TRY(cudaEventSynchronize(ctx->counted[i]));
+        if (first_error == SI_OK && ctx->herr[4 * i] != 0) first_error = static_cast<si_status>(ctx->herr[4 * i]);
+        const uint64_t ci = std::min(ctx->hcount[i], out_at[i + 1] - out_at[i]);
         if (h_out && ci) {
-            SI_CUDA_TRY(cudaStreamWaitEvent(st.down, st.counted[i], 0));
-            SI_CUDA_TRY(cudaMemcpyAsync(h_out + total, dOut + out_at[i], ci * 4, cudaMemcpyDeviceToHost, st.down));
+            SI_CUDA_TRY(cudaStreamWaitEvent(ctx->down, ctx->counted[i], 0));
+            SI_CUDA_TRY(cudaMemcpyAsync(h_out + total, dOut + out_at[i], ci * 4, cudaMemcpyDeviceToHost, ctx->down));
         }
-        total += st.hcount[i];
+        total += ctx->hcount[i];
         return SI_OK;
     };
     for (uint32_t i = 0; i < c.n; ++i) {
         const uint64_t a0 = c.a[i], na = c.a[i + 1] - a0, b0 = c.b[i], nb = c.b[i + 1] - b0;
-        SI_CUDA_TRY(cudaStreamWaitEvent(s, st.landed[i], 0));
+        SI_CUDA_TRY(cudaStreamWaitEvent(s, ctx->landed[i], 0));
         const uint64_t cap = out_at[i + 1] - out_at[i];
         const si_status r = si_sisi(dA + a0, na, dB + b0, nb, t, dCount + i, h_out && cap ? dOut + out_at[i] : nullptr,
                                     cap, ws, L.ws, stream);
-        if (r != SI_OK) return r;  // (the destructor waits for the copies in flight)
-        SI_CUDA_TRY(cudaMemcpyAsync(st.hcount + i, dCount + i, 8, cudaMemcpyDeviceToHost, s));
-        SI_CUDA_TRY(cudaEventRecord(st.counted[i], s));
+        if (r != SI_OK) return r;  // (drain waits for the copies in flight)
+        SI_CUDA_TRY(cudaMemcpyAsync(ctx->hcount + i, dCount + i, 8, cudaMemcpyDeviceToHost, s));
+        SI_CUDA_TRY(cudaMemcpyAsync(ctx->herr + 4 * i, ws, 16, cudaMemcpyDeviceToHost, s));
+        SI_CUDA_TRY(cudaEventRecord(ctx->counted[i], s));
         if (i > 0) {
             const si_status d = copy_down(i - 1);
             if (d != SI_OK) return d;
@@ -176,7 +251,26 @@ extern "C" si_status si_sisi_host(const uint32_t* hA, uint64_t nA, const uint32_
     }
     const si_status d = copy_down(c.n - 1);
     if (d != SI_OK) return d;
-    SI_CUDA_TRY(cudaStreamSynchronize(st.down));
+    SI_CUDA_TRY(cudaStreamSynchronize(ctx->down));
     *count = total;
-    return si_workspace_check(ws, stream);
+    return first_error;
+}
+
+extern "C" si_status si_sisi_host(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint64_t nB, si_technique t,
+                                  uint32_t chunks, uint64_t* count, uint32_t* h_out, uint64_t out_cap,
+                                  void* d_workspace, size_t workspace_bytes, si_stream_t stream) {
+    {  // argument errors and empty sets need no context
+        si::Chunks c;
+        si::Layout L;
+        bool done = false;
+        const si_status arg = si::host_args(hA, nA, hB, nB, t, chunks, count, h_out, out_cap, d_workspace,
+                                            workspace_bytes, c, L, done);
+        if (arg != SI_OK || done) return arg;
+    }
+    si_host_ctx* ctx = nullptr;
+    si_status st = si_host_ctx_create(&ctx);
+    if (st != SI_OK) return st;
+    st = si_sisi_host_ctx(ctx, hA, nA, hB, nB, t, chunks, count, h_out, out_cap, d_workspace, workspace_bytes, stream);
+    si_host_ctx_destroy(ctx);
+    return st;
 }

@@ -44,11 +44,21 @@ private:
     cudaStream_t stream_;
 };
 
-// ---- single-pair tile pipeline (si_sisi_ip.cu) ----
+// ---- single-pair tile pipeline (si_sisi_ip.cu, si_sisi_bitmap.cu) ----
 // inner: 0 = merge path (technique ip), 1 = the bitmap engine (technique
-// bitmap: two bitmaps per tile AND-ed, bm_stage_kernel), 2 = hash probe
+// bitmap: per-warp bitmap build + probe, si_sisi_bitmap.cu), 2 = hash probe
 // (technique hi).  The bitmap engine's workspace is larger (its scratch array).
 size_t ip_workspace_size(uint64_t nA, uint64_t nB, int inner = 0);
+// Value-pivot split of (A, B) at every S-th element of each set into
+// split_a/split_b[nA/S + nB/S + 2] (rounded up); also clears zero[0, nzero)
+// and *d_count.  Lets the next kernel on the stream start early (programmatic
+// dependent launch); that kernel must execute griddepcontrol.wait first.
+si_status pivot_split(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t S,
+                      uint64_t* split_a, uint64_t* split_b, uint64_t* zero, uint64_t nzero, uint64_t* d_count,
+                      cudaStream_t stream);
+size_t bm_workspace_size(uint64_t nA, uint64_t nB);
+si_status bm_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
+                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream);
 // SI_TECH_AUTO searches the smaller set in the larger (obs) when the sizes
 // differ by more than this factor.
 constexpr uint64_t kSkewRatio = 64;

@@ -7,12 +7,12 @@
 // re-designed for B200:
 //
 //  * Grid level: instead of one 32-thread warp probe per diagonal per pair,
-//    tiles are cut at VALUE pivots.  Every S-th element of A and of B is a
-//    pivot (S = 6144); a pivot's exact position in the other set is found with
-//    one bounded binary search inside an S-element window that the sample
-//    merge identifies.  Consecutive pivots bound a tile to <= S elements of
-//    each set, and because a tile boundary is a value, an equal pair is never
-//    split across tiles (no "augmentation" atomic, quirk of
+//    tiles are cut at VALUE pivots (pivot_split, si_sisi_bitmap.cu).  Every
+//    S-th element of A and of B is a pivot (S = 6144); a pivot's rank in the
+//    merged pivot order and its exact position in the other set are found by
+//    warp-cooperative searches.  Consecutive pivots bound a tile to <= S
+//    elements of each set, and because a tile boundary is a value, an equal
+//    pair is never split across tiles (no "augmentation" atomic, quirk of
 //    include/helpers.cuh:121-124).
 //  * Staging: each tile's A and B ranges are copied into shared memory by the
 //    bulk-copy (TMA) engine as their 16-byte aligned supersets (every block
@@ -25,10 +25,8 @@
 //    accumulates tile counts into 256 spread partial sums.
 //
 // Technique bitmap (and auto for pairs of similar size) shares the pivot
-// split (S = 16384) and then runs its own engine, bm_stage_kernel: two
-// bitmaps per tile AND-ed, per-tile counts, a scan and a copy (no look-back).
+// split and runs its own engine (si_sisi_bitmap.cu).
 #include <algorithm>
-#include <cub/device/device_scan.cuh>
 
 #include "si_device.cuh"
 #include "si_internal.h"
@@ -42,12 +40,11 @@ constexpr int kPartials = 256;
 constexpr uint64_t kFlagAgg = 1ull << 62;
 constexpr uint64_t kFlagInc = 2ull << 62;
 constexpr uint64_t kValMask = (1ull << 62) - 1;
-constexpr uint64_t kPoison = ~0ull;
 
 // Workspace layout.  Offsets in bytes from the workspace base.
 struct Layout {
-    uint64_t nSA = 0, nSB = 0, nTiles = 0;
-    size_t off_status = 0, off_split_a = 0, off_split_b = 0, off_sa = 0, off_sb = 0, total = 0;
+    uint64_t nTiles = 0;
+    size_t off_status = 0, off_split_a = 0, off_split_b = 0, total = 0;
 };
 // Header: [0] u32 error word, [4] u32 error site, [8] u32 error detail,
 // [12] u32 sites that gave up, [16] u32 group ticket,
@@ -56,9 +53,7 @@ constexpr size_t kOffTicket = 16, kOffPartials = 64;
 
 Layout make_layout(uint64_t nA, uint64_t nB, uint64_t S) {
     Layout L;
-    L.nSA = (nA + S - 1) / S;
-    L.nSB = (nB + S - 1) / S;
-    L.nTiles = L.nSA + L.nSB + 1;
+    L.nTiles = (nA + S - 1) / S + (nB + S - 1) / S + 1;
     size_t o = align_up(kOffPartials + 8 * kPartials, 256);
     L.off_status = o;
     o = align_up(o + L.nTiles * 8, 256);
@@ -66,97 +61,8 @@ Layout make_layout(uint64_t nA, uint64_t nB, uint64_t S) {
     o = align_up(o + (L.nTiles + 1) * 8, 256);
     L.off_split_b = o;
     o = align_up(o + (L.nTiles + 1) * 8, 256);
-    L.off_sa = o;
-    o = align_up(o + L.nSA * 4, 256);
-    L.off_sb = o;
-    o = align_up(o + L.nSB * 4, 256);
     L.total = o;
     return L;
-}
-
-__device__ __forceinline__ uint64_t lower_bound_g(const uint32_t* __restrict__ x, uint64_t n, uint32_t v) {
-    uint64_t lo = 0, hi = n;  // #(x < v)
-    while (lo < hi) {
-        uint64_t mid = (lo + hi) >> 1;
-        if (__ldg(x + mid) < v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ uint64_t upper_bound_g(const uint32_t* __restrict__ x, uint64_t n, uint32_t v) {
-    uint64_t lo = 0, hi = n;  // #(x <= v)
-    while (lo < hi) {
-        uint64_t mid = (lo + hi) >> 1;
-        if (__ldg(x + mid) <= v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
-// K1: gather the pivot samples, clear the header + tile status words, poison
-// the split table (so a hole left by unsorted input is detected, not used).
-__global__ void ip_prepare_kernel(const uint32_t* __restrict__ A, const uint32_t* __restrict__ B,
-                                  uint32_t* __restrict__ sa, uint64_t nSA, uint32_t* __restrict__ sb, uint64_t nSB,
-                                  uint64_t* __restrict__ zero, uint64_t nzero, uint64_t* __restrict__ split_a,
-                                  uint64_t* __restrict__ split_b, uint64_t nsplit, uint64_t* __restrict__ d_count,
-                                  uint64_t S) {
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    const uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t0 == 0) *d_count = 0;
-    for (uint64_t k = t0; k < nSA; k += stride) sa[k] = __ldg(A + k * S);
-    for (uint64_t k = t0; k < nSB; k += stride) sb[k] = __ldg(B + k * S);
-    for (uint64_t k = t0; k < nzero; k += stride) zero[k] = 0;
-    for (uint64_t k = t0; k < nsplit; k += stride) {
-        split_a[k] = kPoison;
-        split_b[k] = kPoison;
-    }
-}
-
-// K2: one thread per pivot.  Pivot p (A sample k or B sample j) gets its rank
-// u in the merged sample order (ties: A sample first) and its exact split
-// (#A < v, #B < v), stored at split[u + 1].  split[0] = (0,0) and
-// split[nSA + nSB + 1] = (nA, nB) close the table.
-__global__ void ip_split_kernel(const uint32_t* __restrict__ A, uint64_t nA, const uint32_t* __restrict__ B,
-                                uint64_t nB, const uint32_t* __restrict__ sa, uint64_t nSA,
-                                const uint32_t* __restrict__ sb, uint64_t nSB, uint64_t* __restrict__ split_a,
-                                uint64_t* __restrict__ split_b, uint64_t S) {
-    const uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint64_t nP = nSA + nSB;
-    if (p == 0) {
-        split_a[0] = 0;
-        split_b[0] = 0;
-        split_a[nP + 1] = nA;
-        split_b[nP + 1] = nB;
-    }
-    if (p >= nP) return;
-    if (p < nSA) {
-        const uint64_t k = p;
-        const uint32_t v = __ldg(sa + k);
-        const uint64_t j = lower_bound_g(sb, nSB, v);  // B samples < v
-        uint64_t lbB = 0;
-        if (j > 0) {  // B[(j-1)S] < v <= B[jS]  =>  #B<v in ((j-1)S, jS]
-            const uint64_t lo = (j - 1) * S + 1;
-            const uint64_t hi = min(j * S, nB);
-            lbB = lo + lower_bound_g(B + lo, hi > lo ? hi - lo : 0, v);
-        }
-        split_a[k + j + 1] = k * S;
-        split_b[k + j + 1] = lbB;
-    } else {
-        const uint64_t j = p - nSA;
-        const uint32_t v = __ldg(sb + j);
-        const uint64_t i = upper_bound_g(sa, nSA, v);  // A samples <= v
-        uint64_t lbA = 0;
-        if (i > 0) {
-            if (__ldg(sa + i - 1) == v) {
-                lbA = (i - 1) * S;
-            } else {  // A[(i-1)S] < v < A[iS]
-                const uint64_t lo = (i - 1) * S + 1;
-                const uint64_t hi = min(i * S, nA);
-                lbA = lo + lower_bound_g(A + lo, hi > lo ? hi - lo : 0, v);
-            }
-        }
-        split_a[i + j + 1] = lbA;
-        split_b[i + j + 1] = j * S;
-    }
 }
 
 // K3: persistent, warp-specialised tile pipeline.
@@ -288,7 +194,7 @@ __device__ __forceinline__ uint64_t look_back(uint64_t* status, uint64_t t, uint
 // owns as a bit mask over a contiguous run of one staged set: the matched
 // values are src[start + x] for every set bit x, in ascending order, and the
 // runs of consecutive threads are consecutive.
-// (kBitmapProbe selects the separate bitmap engine, bm_stage_kernel, below.)
+// (kBitmapProbe selects the separate bitmap engine of si_sisi_bitmap.cu.)
 enum Inner { kMergePath = 0, kBitmapProbe = 1, kHashProbe = 2 };
 
 struct ThreadMatches {
@@ -696,492 +602,27 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     }
 }
 
-// ---------------------------------------------------------------------------
-// Technique bitmap: three steps after the pivot split, with no ordering
-// between tiles (no look-back).
-//
-//  K3b  bm_stage_kernel, persistent, one CTA of 32 warps per SM.  Warp 31
-//       stages tiles (ticket order) into a shared-memory ring with bulk
-//       copies, several tiles ahead; warps 0-30 take them in turn.  Both parts
-//       of a tile become bitmaps of the value range they share, [lo, hi] =
-//       [max of the firsts, min of the lasts] (16-byte shared loads, one
-//       predicated shared atomic OR per value); the AND of the two bitmaps is the tile's
-//       intersection, already in value order.  Each thread takes a run of
-//       words, counts its bits; a block scan places the runs and the threads
-//       write lo + bit index of every set bit to scratch[tile's first Y
-//       element + rank] and the tile's count to tile_count.  A tile whose
-//       shared range exceeds the bitmaps searches each Y element in the
-//       staged X part instead (one thread per run of Y elements).  Two bitmap
-//       pairs alternate between tiles, and the pass that reads a tile's words
-//       clears them: one barrier of the 31 warps per tile (two with element
-//       output, for the block scan).
-//  K4b  exclusive scan of the tile counts (CUB), total into d_count.
-//  K5b  bm_copy_kernel: every tile's hits from scratch to their offset (a warp per tile).
-// Count-only mode runs K3b alone and adds the hits into d_count.
-// Extra traffic over the algorithmic bytes: the matches written and read once
-// more through the scratch array.
-constexpr uint64_t kBmS = 16384;                // pivot stride of the bitmap tiles
-constexpr int kBmWarps = 31;                    // warps that build and intersect
-constexpr int kBmConsumers = kBmWarps * 32;
-constexpr int kBmBlock = kBmConsumers + 32;     // + the staging warp
-constexpr uint32_t kBmWords = 4096;             // per bitmap: a range of up to 131072 values (16 KiB)
-constexpr uint32_t kBmRing = 40960;             // u32: 160 KiB, about 2.5 tiles of 2 x 8192 elements
-constexpr int kBmSlots = 8;
-constexpr uint32_t kBmBar = 1;                  // named barrier of the 31 warps
-constexpr uint32_t kBmYPerThread = (kBmS + kBmConsumers - 1) / kBmConsumers;  // search fallback
-constexpr size_t kBmSmem = size_t(4 * kBmWords + kBmRing) * sizeof(uint32_t);
-static_assert(2 * (kBmS + 4) <= kBmRing, "one tile's aligned supersets must fit the ring");
-static_assert(kBmYPerThread <= 32, "search fallback: one 32-bit hit mask per thread");
-
-struct BmDesc {
-    uint64_t y0;          // first Y element of the tile (its scratch base)
-    uint32_t tile;
-    uint32_t offX, offY;  // ring index of element 0 of the staged X / Y part
-    uint32_t misX, misY;  // element 0's position in its 16-byte block
-    uint32_t nx, ny;
-};
-
-// Sets the bits of the values of both staged parts that lie in [lo, lo + span].
-// A part is read as 16-byte groups of its staged superset, group g holding
-// elements 4 g - mis ... 4 g - mis + 3.  Only a part's first and last group hold
-// words outside [0, n); four threads take those through a checked path.  The
-// interior groups of both parts form one index space dealt round-robin over
-// the threads (one predicated shared atomic OR per value), so every thread
-// gets the same number of groups to within one.
-__device__ __forceinline__ void bm_set(uint32_t* bm, uint32_t o, uint32_t span) {
-    if (o <= span) atomicOr(bm + (o >> 5), 1u << (o & 31));
-}
-__device__ __forceinline__ void bm_edge(const uint32_t* s, uint32_t mis, uint32_t n, uint32_t lo, uint32_t span,
-                                        uint32_t* bm, uint32_t g) {
-    const uint4 v4 = reinterpret_cast<const uint4*>(s - mis)[g];
-    const uint32_t vv[4] = {v4.x, v4.y, v4.z, v4.w};
-    const int e0 = static_cast<int>(4 * g) - static_cast<int>(mis);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int e = e0 + q;
-        if (e >= 0 && e < static_cast<int>(n)) bm_set(bm, vv[q] - lo, span);
-    }
-}
-__device__ __forceinline__ void bm_build(const uint32_t* sx, uint32_t misX, uint32_t nx, uint32_t* bx,
-                                         const uint32_t* sy, uint32_t misY, uint32_t ny, uint32_t* by, uint32_t lo,
-                                         uint32_t span, int tid) {
-    const uint32_t ngx = (nx + misX + 3) / 4, ngy = (ny + misY + 3) / 4;
-    // the edge groups go to the last threads, which get no more interior groups than the others
-    if (tid == kBmConsumers - 1 && ngx > 0) bm_edge(sx, misX, nx, lo, span, bx, 0);
-    if (tid == kBmConsumers - 2 && ngx > 1) bm_edge(sx, misX, nx, lo, span, bx, ngx - 1);
-    if (tid == kBmConsumers - 3 && ngy > 0) bm_edge(sy, misY, ny, lo, span, by, 0);
-    if (tid == kBmConsumers - 4 && ngy > 1) bm_edge(sy, misY, ny, lo, span, by, ngy - 1);
-    const uint32_t ix = ngx > 2 ? ngx - 2 : 0u, iy = ngy > 2 ? ngy - 2 : 0u;
-    const uint4* gx = reinterpret_cast<const uint4*>(sx - misX) + 1;
-    const uint4* gy = reinterpret_cast<const uint4*>(sy - misY) + 1;
-#pragma unroll 2
-    for (uint32_t c = tid; c < ix + iy; c += kBmConsumers) {
-        const bool isx = c < ix;
-        const uint4 v4 = *(isx ? gx + c : gy + (c - ix));
-        uint32_t* bm = isx ? bx : by;
-        bm_set(bm, v4.x - lo, span);
-        bm_set(bm, v4.y - lo, span);
-        bm_set(bm, v4.z - lo, span);
-        bm_set(bm, v4.w - lo, span);
-    }
-}
-
-template <bool kOut>
-__global__ void __launch_bounds__(kBmBlock, 1) bm_stage_kernel(
-    const uint32_t* __restrict__ X, uint64_t nX, const uint32_t* __restrict__ Y, uint64_t nY,
-    const uint64_t* __restrict__ split_x, const uint64_t* __restrict__ split_y, uint64_t nTiles,
-    unsigned char* __restrict__ ws, uint32_t* __restrict__ tile_count, uint32_t* __restrict__ scratch,
-    uint64_t* __restrict__ d_count) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    uint32_t* bms = smem;                  // 2 pairs (X, Y) of kBmWords
-    uint32_t* ring = smem + 4 * kBmWords;  // kBmRing
-    __shared__ __align__(8) uint64_t full[kBmSlots], empty[kBmSlots];
-    __shared__ BmDesc desc[kBmSlots];
-    __shared__ uint64_t s_end[kBmSlots];  // staging lane: ring end (virtual) of the tile in each slot
-    __shared__ uint32_t s_warp[2][32];    // per tile parity: hits of each warp
-    __shared__ unsigned long long s_hits;
-    uint32_t* err = reinterpret_cast<uint32_t*>(ws);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // bitmaps are all zero between uses: the pass that reads a tile's words clears them
-    for (uint32_t w = tid; w < 4 * kBmWords; w += kBmBlock) bms[w] = 0u;
-    if (tid == 0) {
-        for (int i = 0; i < kBmSlots; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], kBmWarps);
-        }
-        s_hits = 0;
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    if (warp == kBmWarps) {
-        // ------------------------------------------------------- staging --
-        if (lane != 0) return;
-        uint32_t* ticket = reinterpret_cast<uint32_t*>(ws + kOffTicket);
-        uint64_t head = 0, released = 0;  // virtual ring offsets
-        uint32_t k = 0, k_rel = 0;        // tiles staged / tiles released by every warp
-        auto wait_release = [&]() -> bool {
-            const uint32_t sl = k_rel % kBmSlots;
-            if (!mbar_wait_bounded(&empty[sl], (k_rel / kBmSlots) & 1u, err, 12, k_rel)) return false;
-            released = s_end[sl];
-            ++k_rel;
-            return true;
-        };
-        // tickets two tiles ahead, split entries one tile ahead
-        uint64_t t = atomicAdd(ticket, 1u), t_next = atomicAdd(ticket, 1u);
-        uint64_t x0 = 0, x1 = 0, y0 = 0, y1 = 0;
-        if (t < nTiles) {
-            x0 = split_x[t];
-            x1 = split_x[t + 1];
-            y0 = split_y[t];
-            y1 = split_y[t + 1];
-        }
-        bool alive = true;
-        for (;;) {
-            uint64_t t_after = nTiles, nx0 = 0, nx1 = 0, ny0 = 0, ny1 = 0;
-            if (t < nTiles) {
-                t_after = atomicAdd(ticket, 1u);
-                if (t_next < nTiles) {
-                    nx0 = split_x[t_next];
-                    nx1 = split_x[t_next + 1];
-                    ny0 = split_y[t_next];
-                    ny1 = split_y[t_next + 1];
-                }
-            }
-            const uint32_t slot = k % kBmSlots;
-            while (alive && k_rel + kBmSlots <= k) alive = wait_release();
-            if (!alive) break;
-            if (t >= nTiles) {  // end marker: never released, not counted in k
-                desc[slot].tile = kEndTile;
-                mbar_arrive(&full[slot]);
-                break;
-            }
-            const bool ok = x0 <= x1 && x1 <= nX && x1 - x0 <= kBmS && y0 <= y1 && y1 <= nY && y1 - y0 <= kBmS;
-            if (!ok) {
-                record_error(err, SI_ERR_INVALID_INPUT);
-                x0 = x1 = y0 = y1 = 0;
-            }
-            // 16-byte aligned supersets of the parts: every block copied holds
-            // an element of the part, so no byte outside the sets' blocks is read
-            const uintptr_t xlo = reinterpret_cast<uintptr_t>(X + x0) & ~uintptr_t(15);
-            const uintptr_t ylo = reinterpret_cast<uintptr_t>(Y + y0) & ~uintptr_t(15);
-            const uint32_t bytesX =
-                x1 > x0 ? static_cast<uint32_t>(((reinterpret_cast<uintptr_t>(X + x1) + 15) & ~uintptr_t(15)) - xlo) : 0u;
-            const uint32_t bytesY =
-                y1 > y0 ? static_cast<uint32_t>(((reinterpret_cast<uintptr_t>(Y + y1) + 15) & ~uintptr_t(15)) - ylo) : 0u;
-            const uint32_t need = (bytesX + bytesY) / 4;
-            // a tile never wraps; it is placed once it overlaps no live tile
-            const uint64_t phys = head % kBmRing;
-            if (phys + need > kBmRing) head += kBmRing - phys;
-            while (alive && k_rel < k && head + need - released > kBmRing) alive = wait_release();
-            if (!alive) break;
-            const uint32_t pos = static_cast<uint32_t>(head % kBmRing);
-            head += need;
-            s_end[slot] = head;
-            BmDesc& d = desc[slot];
-            d.tile = static_cast<uint32_t>(t);
-            d.y0 = y0;
-            d.misX = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(X + x0) & 15u) >> 2);
-            d.misY = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(Y + y0) & 15u) >> 2);
-            d.offX = pos + d.misX;
-            d.offY = pos + bytesX / 4 + d.misY;
-            d.nx = static_cast<uint32_t>(x1 - x0);
-            d.ny = static_cast<uint32_t>(y1 - y0);
-            mbar_arrive_expect_tx(&full[slot], bytesX + bytesY);
-            if (bytesX) bulk_g2s(ring + pos, reinterpret_cast<const void*>(xlo), bytesX, &full[slot]);
-            if (bytesY) bulk_g2s(ring + pos + bytesX / 4, reinterpret_cast<const void*>(ylo), bytesY, &full[slot]);
-            ++k;
-            t = t_next;
-            t_next = t_after;
-            x0 = nx0;
-            x1 = nx1;
-            y0 = ny0;
-            y1 = ny1;
-        }
-        // the copies in flight land before the CTA may exit: normally every
-        // staged tile (k of them, the end marker not counted) is released; if
-        // a wait gave up, wait for the copies themselves (bounded)
-        while (alive && k_rel < k) alive = wait_release();
-        for (uint32_t q = k_rel; q < k; ++q) mbar_wait_bounded(&full[q % kBmSlots], (q / kBmSlots) & 1u, err, 13, q);
-        return;
-    }
-
-    // ----------------------------------------------- build + intersect --
-    uint32_t my_hits = 0;
-    for (uint32_t k = 0;; ++k) {
-        const uint32_t slot = k % kBmSlots;
-        if (!mbar_wait_bounded(&full[slot], (k / kBmSlots) & 1u, err, 14, k)) break;
-        const BmDesc d = desc[slot];
-        if (d.tile == kEndTile) break;
-        const uint32_t par = k & 1u;
-        uint32_t* bx = bms + par * 2 * kBmWords;
-        uint32_t* by = bx + kBmWords;
-        const uint32_t* sx = ring + d.offX;
-        const uint32_t* sy = ring + d.offY;
-        const uint32_t nx = d.nx, ny = d.ny;
-        bool any = nx > 0 && ny > 0;
-        uint32_t lo = 0, span = 0;
-        if (any) {
-            lo = max(sx[0], sy[0]);
-            const uint32_t hi = min(sx[nx - 1], sy[ny - 1]);
-            any = lo <= hi;
-            span = hi - lo;
-        }
-        const bool fits = any && span < kBmWords * 32u;
-        const uint32_t words = fits ? (span >> 5) + 1 : 0u;
-        // Building into this pair needs no barrier first: it was cleared by
-        // the pass over tile k - 2, which every warp finished before it
-        // arrived at the barrier of tile k - 1 below.
-        // this thread's hits: bits of its words (bitmaps) or of its Y run (search)
-        const uint32_t wpt = (words + kBmConsumers - 1) / kBmConsumers;
-        const uint32_t w0 = min(words, tid * wpt), w1 = min(words, w0 + wpt);
-        const uint32_t yrun = (ny + kBmConsumers - 1) / kBmConsumers;  // <= kBmYPerThread
-        const uint32_t j0 = min(ny, tid * yrun), j1 = min(ny, j0 + yrun);
-        uint32_t ymask = 0;
-        if (fits) {
-            bm_build(sx, d.misX, nx, bx, sy, d.misY, ny, by, lo, span, tid);
-        } else if (any) {
-            for (uint32_t j = j0; j < j1; ++j) {
-                const uint32_t v = sy[j];
-                uint32_t l = 0, len = nx;  // #(sx < v)
-                while (len > 0) {
-                    const uint32_t half = len >> 1;
-                    const bool less = sx[l + half] < v;
-                    l = less ? l + half + 1 : l;
-                    len = less ? len - half - 1 : half;
-                }
-                if (l < nx && sx[l] == v) ymask |= 1u << (j - j0);
-            }
-        }
-        named_barrier(kBmBar, kBmConsumers);
-        // the ring slot is released once no thread reads it any more: now,
-        // unless the search fallback still writes Y values below
-        const bool late_release = kOut && !fits && any;
-        if (!late_release) {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[slot]);
-        }
-        uint32_t h = __popc(ymask);
-        for (uint32_t w = w0; w < w1; ++w) {
-            h += __popc(bx[w] & by[w]);
-            if constexpr (!kOut) {
-                bx[w] = 0u;
-                by[w] = 0u;
-            }
-        }
-        if constexpr (kOut) {
-            const uint32_t incl = warp_inclusive_scan(h);
-            if (lane == 31) s_warp[par][warp] = incl;
-            named_barrier(kBmBar, kBmConsumers);
-            const uint32_t wt = lane < kBmWarps ? s_warp[par][lane] : 0u;
-            const uint32_t wincl = warp_inclusive_scan(wt);
-            const uint32_t wbefore = __shfl_sync(kFullMask, wincl - wt, warp);
-            const uint32_t total = __shfl_sync(kFullMask, wincl, 31);
-            if (tid == 0) tile_count[d.tile] = total;
-            uint32_t* dst = scratch + d.y0 + wbefore + (incl - h);
-            if (ymask) {
-                for (uint32_t m = ymask; m; m &= m - 1) *dst++ = sy[j0 + __ffs(m) - 1];
-            } else {
-                for (uint32_t w = w0; w < w1; ++w) {
-                    uint32_t m = bx[w] & by[w];
-                    bx[w] = 0u;
-                    by[w] = 0u;
-                    for (; m; m &= m - 1) *dst++ = lo + 32 * w + (__ffs(m) - 1);
-                }
-            }
-        }
-        if (late_release) {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[slot]);
-        }
-        my_hits += h;
-    }
-    if constexpr (!kOut) {
-        const uint32_t wsum = __reduce_add_sync(kFullMask, my_hits);
-        if (lane == 0 && wsum) atomicAdd(&s_hits, static_cast<unsigned long long>(wsum));
-        named_barrier(kBmBar, kBmConsumers);
-        if (tid == 0 && s_hits) atomicAdd(reinterpret_cast<unsigned long long*>(d_count), s_hits);
-    }
-}
-
-// K5b: tile t's tile_count[t] hits at scratch[split_y[t] ...] go to
-// out[tile_offset[t] ...].  One warp per tile, grid-stride over the tiles; the
-// next tile's count and offsets are loaded while the current one is copied,
-// and each lane keeps 8 loads in flight.
-constexpr int kBmCopyUnroll = 8;
-__global__ void __launch_bounds__(256) bm_copy_kernel(const uint32_t* __restrict__ tile_count,
-                                                      const uint64_t* __restrict__ tile_offset,
-                                                      const uint64_t* __restrict__ split_y, uint64_t nTiles,
-                                                      const uint32_t* __restrict__ scratch, uint32_t* __restrict__ out,
-                                                      uint64_t out_cap, uint32_t* err) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x / 32);
-    uint64_t t = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
-    bool overflow = false;
-    uint32_t n = 0;
-    uint64_t o = 0, src = 0;
-    if (t < nTiles) {
-        n = tile_count[t];
-        o = tile_offset[t];
-        src = split_y[t];
-    }
-    while (t < nTiles) {  // warp-uniform
-        const uint64_t tn = t + warps;
-        uint32_t n2 = 0;
-        uint64_t o2 = 0, src2 = 0;
-        if (tn < nTiles) {
-            n2 = tile_count[tn];
-            o2 = tile_offset[tn];
-            src2 = split_y[tn];
-        }
-        for (uint32_t i0 = 0; i0 < n; i0 += 32 * kBmCopyUnroll) {
-            uint32_t v[kBmCopyUnroll];
-#pragma unroll
-            for (int u = 0; u < kBmCopyUnroll; ++u) {
-                const uint32_t i = i0 + 32 * u + lane;
-                v[u] = i < n ? __ldg(scratch + src + i) : 0u;
-            }
-#pragma unroll
-            for (int u = 0; u < kBmCopyUnroll; ++u) {
-                const uint32_t i = i0 + 32 * u + lane;
-                if (i < n) {
-                    if (o + i < out_cap) out[o + i] = v[u];
-                    else overflow = true;
-                }
-            }
-        }
-        t = tn;
-        n = n2;
-        o = o2;
-        src = src2;
-    }
-    if (overflow) record_error(err, SI_ERR_OUTPUT_OVERFLOW, 9, 0);
-}
-
-__global__ void bm_total_kernel(const uint32_t* __restrict__ tile_count, const uint64_t* __restrict__ tile_offset,
-                                uint64_t nTiles, uint64_t* __restrict__ d_count) {
-    if (nTiles) *d_count = tile_offset[nTiles - 1] + tile_count[nTiles - 1];
-}
-
-// Workspace of technique bitmap: the tile tables of make_layout(kBmS), then
-// tile counts (u32) and their offsets (u64), the scratch array of the hits
-// (as long as the smaller set), and the scan's temporary storage.
-struct BmLayout {
-    Layout L;
-    uint64_t nY = 0;
-    size_t off_count = 0, off_offset = 0, off_scratch = 0, off_cub = 0, cub_bytes = 0, total = 0;
-};
-
-BmLayout make_bm_layout(uint64_t nA, uint64_t nB) {
-    BmLayout B;
-    B.L = make_layout(nA, nB, kBmS);
-    B.nY = std::min(nA, nB);
-    const uint64_t n = B.L.nTiles;
-    size_t o = B.L.total;
-    B.off_count = o;   o = align_up(o + n * 4, 256);
-    B.off_offset = o;  o = align_up(o + n * 8, 256);
-    B.off_scratch = o; o = align_up(o + B.nY * 4, 256);
-    // without a device to ask, a bound of 1 MiB
-    size_t bytes = 0;
-    if (n > 0x7fffffffull ||
-        cub::DeviceScan::ExclusiveScan(nullptr, bytes, static_cast<const uint32_t*>(nullptr),
-                                       static_cast<uint64_t*>(nullptr), cub::Sum(), uint64_t(0),
-                                       static_cast<int>(std::min<uint64_t>(n, 0x7fffffff))) != cudaSuccess)
-        bytes = 1u << 20;
-    cudaGetLastError();  // a failed query leaves no sticky error behind
-    B.cub_bytes = align_up(bytes, 256);
-    B.off_cub = o;
-    B.total = o + B.cub_bytes;
-    return B;
-}
-
 }  // namespace
 
 size_t ip_workspace_size(uint64_t nA, uint64_t nB, int inner) {
-    return inner == kBitmapProbe ? make_bm_layout(nA, nB).total : make_layout(nA, nB, kS).total;
+    return inner == kBitmapProbe ? bm_workspace_size(nA, nB) : make_layout(nA, nB, kS).total;
 }
 
 si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
                   uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream, int inner) {
-    const bool bitmap = inner == kBitmapProbe;
-    const uint64_t S = bitmap ? kBmS : kS;
-    const Layout L = make_layout(nA, nB, S);
-    if (ws_bytes < (bitmap ? make_bm_layout(nA, nB).total : L.total)) return SI_ERR_WORKSPACE_TOO_SMALL;
+    if (inner == kBitmapProbe) return bm_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, ws, ws_bytes, stream);
+    const Layout L = make_layout(nA, nB, kS);
+    if (ws_bytes < L.total) return SI_ERR_WORKSPACE_TOO_SMALL;
     if (L.nTiles > 0x7fffffffull) return SI_ERR_INVALID_ARGUMENT;
     unsigned char* w = static_cast<unsigned char*>(ws);
-    uint32_t* sa = reinterpret_cast<uint32_t*>(w + L.off_sa);
-    uint32_t* sb = reinterpret_cast<uint32_t*>(w + L.off_sb);
     uint64_t* split_a = reinterpret_cast<uint64_t*>(w + L.off_split_a);
     uint64_t* split_b = reinterpret_cast<uint64_t*>(w + L.off_split_b);
     uint64_t* status = reinterpret_cast<uint64_t*>(w + L.off_status);
-
-    const uint64_t nzero = L.off_split_a / 8;
-    const uint64_t work1 = std::max(std::max(L.nSA, L.nSB), std::max(nzero, L.nTiles + 1));
-    const unsigned grid1 =
-        static_cast<unsigned>(std::min<uint64_t>((work1 + 255) / 256, static_cast<uint64_t>(sm_count()) * 8));
-    {
-    PhaseTimer timer("sisi_prepare", stream);
-    ip_prepare_kernel<<<grid1, 256, 0, stream>>>(dA, dB, sa, L.nSA, sb, L.nSB, reinterpret_cast<uint64_t*>(w), nzero,
-                                                 split_a, split_b, L.nTiles + 1, d_count, S);
-    SI_LAUNCH_CHECK("ip_prepare_kernel");
-    }
-
-    const uint64_t nP = L.nSA + L.nSB;
-    const unsigned grid2 = static_cast<unsigned>(std::max<uint64_t>(1, (nP + 255) / 256));
-    {
-    PhaseTimer timer("sisi_split", stream);
-    ip_split_kernel<<<grid2, 256, 0, stream>>>(dA, nA, dB, nB, sa, L.nSA, sb, L.nSB, split_a, split_b, S);
-    SI_LAUNCH_CHECK("ip_split_kernel");
-    }
-
-    if (bitmap) {
-        const BmLayout B = make_bm_layout(nA, nB);
-        // the smaller set (Y) indexes the scratch array: a tile has at most
-        // as many hits as Y elements
-        const bool swap = nA < nB;
-        const uint32_t* X = swap ? dB : dA;
-        const uint32_t* Y = swap ? dA : dB;
-        const uint64_t nX = swap ? nB : nA, nY = swap ? nA : nB;
-        const uint64_t* split_x = swap ? split_b : split_a;
-        const uint64_t* split_y = swap ? split_a : split_b;
-        uint32_t* tile_count = reinterpret_cast<uint32_t*>(w + B.off_count);
-        uint64_t* tile_offset = reinterpret_cast<uint64_t*>(w + B.off_offset);
-        uint32_t* scratch = reinterpret_cast<uint32_t*>(w + B.off_scratch);
-        auto probe = [&](auto kernel) -> si_status {
-            SI_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(kBmSmem)));
-            int per_sm = 0;
-            SI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBmBlock, kBmSmem));
-            if (per_sm < 1) return SI_ERR_UNSUPPORTED;
-            const unsigned grid =
-                static_cast<unsigned>(std::min<uint64_t>(L.nTiles, static_cast<uint64_t>(sm_count()) * per_sm));
-            PhaseTimer timer("sisi_tile", stream);
-            kernel<<<grid, kBmBlock, kBmSmem, stream>>>(X, nX, Y, nY, split_x, split_y, L.nTiles, w, tile_count,
-                                                        scratch, d_count);
-            SI_LAUNCH_CHECK("bm_stage_kernel");
-            return SI_OK;
-        };
-        if (!d_out) return probe(bm_stage_kernel<false>);
-        si_status st = probe(bm_stage_kernel<true>);
-        if (st != SI_OK) return st;
-        {
-            PhaseTimer timer("sisi_scan", stream);
-            size_t bytes = B.cub_bytes;
-            SI_CUDA_TRY(cub::DeviceScan::ExclusiveScan(w + B.off_cub, bytes, tile_count, tile_offset, cub::Sum(),
-                                                       uint64_t(0), static_cast<int>(L.nTiles), stream));
-            bm_total_kernel<<<1, 1, 0, stream>>>(tile_count, tile_offset, L.nTiles, d_count);
-            SI_LAUNCH_CHECK("bm_total_kernel");
-        }
-        {
-            PhaseTimer timer("sisi_copy", stream);
-            const unsigned grid = static_cast<unsigned>(
-                std::min<uint64_t>((L.nTiles + 7) / 8, static_cast<uint64_t>(sm_count()) * 8));
-            bm_copy_kernel<<<std::max(grid, 1u), 256, 0, stream>>>(tile_count, tile_offset, split_y, L.nTiles, scratch,
-                                                                   d_out, out_cap, reinterpret_cast<uint32_t*>(w));
-            SI_LAUNCH_CHECK("bm_copy_kernel");
-        }
-        return SI_OK;
-    }
+    // the split kernel also clears the header, the partial counts and the
+    // tiles' look-back status words
+    const si_status sst = pivot_split(dA, nA, dB, nB, kS, split_a, split_b, reinterpret_cast<uint64_t*>(w),
+                                      L.off_split_a / 8, d_count, stream);
+    if (sst != SI_OK) return sst;
 
     const uint64_t nGroups = (L.nTiles + kGroup - 1) / kGroup;
     auto launch = [&](auto kernel, uint32_t* out) -> si_status {

@@ -85,3 +85,28 @@ def test_planted_mistake_is_caught():
     got = oracle.all_pairs(ds.elements, ds.offsets, ds.cardinality, ds.universe, "std").astype(np.uint64)
     got[17] += 1
     assert not np.array_equal(got, expected)
+
+
+@pytest.mark.parametrize("seed,n,hi,lo", [
+    (3, 1 << 16, 1 << 19, 0),          # dense branch (n > U/64)
+    (4, 5000, 1 << 14, 100),           # dense, offset range
+    (1, 1 << 12, 1 << 24, 0),          # sparse branch
+    (7, 1000, (1 << 32), (1 << 32) - (1 << 20)),  # sparse, top of the u32 range
+    (9, 0, 10, 0),
+])
+def test_gen_uniform_equals_engine_generator(seed, n, hi, lo):
+    """The oracle's restated generator yields exactly the engine's sets, so the
+    reference's executables can be run on the engine's inputs without loading
+    the engine's library."""
+    from set_intersection_b200 import generate
+    want = generate.uniform(seed, n, hi, lo)
+    got = oracle.gen_uniform(seed, n, hi, lo)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_write_dataset_matches_format_module(tmp_path):
+    sets = [np.array([1, 5, 9], dtype=np.uint32), np.array([], dtype=np.uint32), np.array([0, 2], dtype=np.uint32)]
+    p1, p2 = tmp_path / "a.bin", tmp_path / "b.bin"
+    oracle.write_dataset(str(p1), sets, 9)
+    fmt.write_dataset(str(p2), fmt.from_sets(sets, universe=9))
+    assert p1.read_bytes() == p2.read_bytes()
