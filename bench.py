@@ -27,8 +27,11 @@ Metric: Gelem/s = (|A| + |B|) / step time.
           library's phase timer over the timed region, against measured HBM;
           phase_avg_ms lists every phase of the step (split, tiles, scan, copy).
   cpu_baseline  the reference's own CPU executable (oracle/_ref/stdintersection,
-          built from the reference sources) on a bounded sample of the same
-          workload, timed by the reference's HostTimer.
+          built from the reference sources) on value-range slices of the same
+          pair, timed by the reference's HostTimer.
+  --impl reference  the same executable on slices of the same pair, built
+          in that process by the oracle's restatement of the engine's seeded
+          generator (the engine's library is never loaded there).
 
 Multi-GPU: the single-pair path is replicas only -- each rank runs its own
 independent pair (no data-path collective); value is the whole-job aggregate.
@@ -129,22 +132,6 @@ def make_pair(name: str):
     return a, b
 
 
-def sample_pair(name: str, budget_elems: int):
-    """A bounded sample with the workload's density: |A'| = |B'| = n' drawn
-    from a universe scaled by n'/n (same per-element merge behaviour)."""
-    from set_intersection_b200 import generate
-    w = WORKLOADS[name]
-    if name == "sisi_skewed":
-        return make_pair(name), "full workload"
-    n = w["n"]
-    ns = int(min(n, max(1 << 16, budget_elems)))
-    ns = 1 << (ns.bit_length() - 1)
-    uni = int(w["universe"] * ns // n)
-    a = generate.uniform(w["seeds"][0] + 100, ns, uni)
-    b = generate.uniform(w["seeds"][1] + 100, ns, uni)
-    return (a, b), f"|A|=|B|=2^{ns.bit_length() - 1} from [0,2^{uni.bit_length() - 1}) (same density as the workload)"
-
-
 # ------------------------------------------------------------------ clocks --
 class ClockSampler:
     """Samples SM clock and clock-event reasons through NVML while running."""
@@ -210,54 +197,108 @@ class ClockSampler:
 
 
 # -------------------------------------------------------------- reference --
-def reference_step_ms(a, b, tmpdir: str) -> float:
-    """One run of the reference's stdintersection on a 2-set dataset file; the
-    reference's own HostTimer figure for the intersection phase."""
+def ref_pair(name: str):
+    """The workload's pair as the reference arm builds it: the oracle's
+    restatement of the engine's seeded generator (oracle.gen_uniform yields the
+    very same sets), so this process never loads the engine's library."""
     import oracle
-    from set_intersection_b200 import dataset as fmt
-    path = os.path.join(tmpdir, "pair.bin")
-    if not os.path.exists(path):
-        fmt.write_dataset(path, fmt.from_sets([a, b], universe=int(max(a[-1], b[-1]))))
-    r = oracle.run_ref("stdintersection", path, threads=os.cpu_count())
-    return r["host_ms"]["std::set intersection"]
+    w = WORKLOADS[name]
+    os.makedirs(CACHE_DIR, exist_ok=True)
+    path = os.path.join(CACHE_DIR, f"{name}.npz")  # the same sets as the engine arm's cache
+    if os.path.exists(path):
+        try:
+            z = np.load(path)
+            return z["a"], z["b"]
+        except Exception:
+            pass
+    a = oracle.gen_uniform(w["seeds"][0], w["n"], w["universe"])
+    b = oracle.gen_uniform(w["seeds"][1], w["n"], w["universe"])
+    tmp = path + f".{os.getpid()}.tmp.npz"
+    np.savez(tmp, a=a, b=b)
+    os.replace(tmp, path)
+    return a, b
 
 
-def port_step_ms(a, b) -> float:
+def ref_slices(a, b, n_slices: int, per_set: int):
+    """n_slices value-range slices of the pair, evenly spaced over it: slice j
+    holds per_set consecutive elements of a from position j |a| / n_slices and
+    the elements of b in the same value range (same density as the pair)."""
+    out = []
+    per_set = min(per_set, a.size // n_slices)
+    for j in range(n_slices):
+        i0 = j * a.size // n_slices
+        i1 = i0 + per_set
+        lo = int(a[i0])
+        j0 = int(np.searchsorted(b, lo, "left"))
+        j1 = int(np.searchsorted(b, int(a[i1]), "left")) if i1 < a.size else b.size
+        out.append((a[i0:i1], b[j0:j1]))
+    return out
+
+
+def ref_sisi_measure(a, b, steps: int, warmup: int, budget_s: float):
+    """The reference's own stdintersection (oracle/_ref, built from
+    src/std_set_intersection.cpp) timed by its HostTimer on slices of the pair:
+    step i runs slice i mod 8, sized so the whole run takes about budget_s.
+    Returns (kind, Gelem/s over the timed steps, description)."""
     import oracle
-    t0 = time.perf_counter()
-    oracle.count(a, b, "std")
-    return (time.perf_counter() - t0) * 1e3
-
-
-def cpu_measure(a, b, steps: int, warmup: int):
-    import oracle
-    kind = "reference" if oracle.ref_binary("stdintersection") else "port"
-    times = []
+    exe = oracle.ref_binary("stdintersection")
+    # about 35 ns per element per run (the reference reads its dataset
+    # element by element, then intersects on one thread)
+    total = int(budget_s / max(1, steps + warmup) / 35e-9)
+    per_set = 1 << max(16, min(27, (total // 2).bit_length() - 1))
+    while per_set > 1 and per_set > a.size // 8:
+        per_set >>= 1
+    slices = ref_slices(a, b, 8, per_set)
+    elems, ms_sum = 0, 0.0
     with tempfile.TemporaryDirectory() as td:
         for i in range(warmup + steps):
-            ms = reference_step_ms(a, b, td) if kind == "reference" else port_step_ms(a, b)
+            sa, sb = slices[i % len(slices)]
+            if exe:
+                path = os.path.join(td, f"slice{i % len(slices)}.bin")
+                if not os.path.exists(path):
+                    oracle.write_dataset(path, [sa, sb], int(max(sa[-1], sb[-1]) if sb.size else sa[-1]))
+                ms = oracle.run_ref("stdintersection", path, threads=os.cpu_count())["host_ms"]["std::set intersection"]
+            else:
+                t0 = time.perf_counter()
+                oracle.count(sa, sb, "std")
+                ms = (time.perf_counter() - t0) * 1e3
             if i >= warmup:
-                times.append(ms)
-    return kind, times
+                elems += sa.size + sb.size
+                ms_sum += ms
+    kind = "reference" if exe else "port"
+    desc = (f"step i: value-range slice i mod 8 of the workload's pair (8 slices evenly spaced over it, "
+            f"2^{per_set.bit_length() - 1} elements of A each plus B's elements in the same range: the same "
+            f"sets and density), {'oracle/_ref/stdintersection --threads nproc (src/std_set_intersection.cpp:58-76; with 2 sets one thread has work), its HostTimer' if exe else 'oracle std::set_intersection port'}; "
+            f"Gelem/s = elements of the timed steps / their summed time")
+    return kind, elems / (ms_sum * 1e-3) / 1e9, desc
+
+
+def sisi_config(args, n_a: int, n_b: int, world: int) -> dict:
+    """The workload's description, the same in both arms' lines."""
+    return {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "materialize": bool(args.materialize),
+            "n_a": int(n_a), "n_b": int(n_b),
+            "l2": "inputs 2 GiB per step > 126 MB L2; no flush" if args.workload == "sisi_large"
+                  else "inputs resident; no flush",
+            "parallelism": f"replicas{world}"}
 
 
 def run_reference_arm(args, rank: int):
     if rank != 0:
         return
-    # sized so that (steps + warmup) runs stay within a few minutes
-    per_step_budget = max(1 << 18, int((1 << 26) * 40 / max(1, args.steps + args.warmup)))
-    (a, b), desc = sample_pair(args.workload, per_step_budget)
-    kind, times = cpu_measure(a, b, args.steps, args.warmup)
-    ms = statistics.median(times)
-    value = (a.size + b.size) / (ms * 1e-3) / 1e9
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.workload == "sisi_skewed":
+        a, b = make_pair(args.workload)  # planted pair: the engine's generator
+    else:
+        a, b = ref_pair(args.workload)
+    kind, value, desc = ref_sisi_measure(a, b, args.steps, args.warmup, budget_s=150.0)
     line = {
         "impl": "reference", "metric": "SISI Gelem/s", "value": value, "unit": "Gelem/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": (a.size + b.size) / (value * 1e9) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"], "technique": "std::set_intersection"},
-        "cpu_baseline": {"value": value, "unit": "Gelem/s", "cores": 1, "kind": kind,
-                         "sample": desc + "; stdintersection --threads nproc: with 2 sets only one thread has work "
-                                          "(src/std_set_intersection.cpp:58-76); median of steps"},
+        "config": sisi_config(args, a.size, b.size, world),
+        "technique": "std::set_intersection",
+        "cpu_baseline": {"value": value, "unit": "Gelem/s", "cores": 1, "kind": kind, "sample": desc},
         "e2e": {"value": value, "unit": "Gelem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -395,23 +436,15 @@ def run_ours(args, rank: int, world: int):
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        (sa, sb), desc = sample_pair(args.workload, 1 << 26)
-        kind, times = cpu_measure(sa, sb, steps=3, warmup=1)
-        cms = statistics.median(times)
-        cpu = {"value": (sa.size + sb.size) / (cms * 1e-3) / 1e9, "unit": "Gelem/s", "cores": 1, "kind": kind,
-               "sample": desc + "; median of 3 runs of the reference's stdintersection (one pair: one thread "
-                                "has work, src/std_set_intersection.cpp:58-76), timed by its HostTimer"}
+        kind, cval, desc = ref_sisi_measure(a, b, steps=3, warmup=1, budget_s=20.0)
+        cpu = {"value": cval, "unit": "Gelem/s", "cores": 1, "kind": kind, "sample": desc}
 
     line = {
         "metric": "SISI Gelem/s", "value": value, "unit": "Gelem/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
-                   "technique": args.technique, "materialize": bool(args.materialize),
-                   "n_a": int(n_a), "n_b": int(n_b), "intersection": c,
-                   "l2": "inputs 2 GiB per step > 126 MB L2; no flush" if args.workload == "sisi_large"
-                         else "inputs resident; no flush",
-                   "parallelism": f"replicas{world}", "parity_vs_oracle": parity},
+        "config": sisi_config(args, n_a, n_b, world),
+        "technique": args.technique, "intersection": c, "parity_vs_oracle": parity,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": kernel, "engine": engine, "alg_bytes_per_launch": alg_bytes,
@@ -970,6 +1003,7 @@ def other_workloads(args) -> list:
         cfg = d.get("config") or {}
         keep = {k: cfg[k] for k in ("technique", "operand", "parity_vs_oracle", "speedup_vs_plain",
                                      "plain_popcount_ms_per_step", "plain_per_pair") if k in cfg}
+        keep.update({k: d[k] for k in ("technique", "parity_vs_oracle") if k in d})
         out.append({"workload": wl, "metric": d["metric"], "value": d["value"], "unit": d["unit"],
                     "ms_per_step": d["ms_per_step"], "steps": d["steps"],
                     "roofline": {k: roof.get(k) for k in ("bound", "achieved", "peak", "unit", "frac", "kernel",

@@ -142,6 +142,16 @@ __device__ __forceinline__ void st_release_shared_u64(uint64_t* p, uint64_t v) {
     asm volatile("st.release.cta.shared::cta.u64 [%0], %1;" ::"r"(smem_addr(p)), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ uint32_t ld_acquire_shared_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_addr(p)) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_shared_u32(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(smem_addr(p)), "r"(v) : "memory");
+}
+
 // 1-D bulk copy global -> shared (TMA engine), completion counted on `bar`.
 // dst and src must be 16-byte aligned and bytes a multiple of 16.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {

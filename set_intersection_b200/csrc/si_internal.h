@@ -50,12 +50,15 @@ private:
 // (technique hi).  The bitmap engine's workspace is larger (its scratch array).
 size_t ip_workspace_size(uint64_t nA, uint64_t nB, int inner = 0);
 // Value-pivot split of (A, B) at every S-th element of each set into
-// split_a/split_b[nA/S + nB/S + 2] (rounded up); also clears zero[0, nzero)
-// and *d_count.  Lets the next kernel on the stream start early (programmatic
-// dependent launch); that kernel must execute griddepcontrol.wait first.
+// split_a/split_b[nA/S + nB/S + 2] (rounded up), through the sample arrays
+// samples_a/samples_b (pivot_samples_bytes in all, two 256-byte aligned
+// parts); also clears zero[0, nzero) and *d_count.  Lets the next kernel on
+// the stream start early (programmatic dependent launch); that kernel must
+// execute griddepcontrol.wait before it reads any of these.
 si_status pivot_split(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t S,
-                      uint64_t* split_a, uint64_t* split_b, uint64_t* zero, uint64_t nzero, uint64_t* d_count,
-                      cudaStream_t stream);
+                      uint64_t* split_a, uint64_t* split_b, uint32_t* samples_a, uint32_t* samples_b,
+                      uint64_t* zero, uint64_t nzero, uint64_t* d_count, cudaStream_t stream);
+size_t pivot_samples_bytes(uint64_t nA, uint64_t nB, uint64_t S);
 size_t bm_workspace_size(uint64_t nA, uint64_t nB);
 si_status bm_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
                   uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream);

@@ -44,7 +44,7 @@ constexpr uint64_t kValMask = (1ull << 62) - 1;
 // Workspace layout.  Offsets in bytes from the workspace base.
 struct Layout {
     uint64_t nTiles = 0;
-    size_t off_status = 0, off_split_a = 0, off_split_b = 0, total = 0;
+    size_t off_status = 0, off_split_a = 0, off_split_b = 0, off_samples = 0, total = 0;
 };
 // Header: [0] u32 error word, [4] u32 error site, [8] u32 error detail,
 // [12] u32 sites that gave up, [16] u32 group ticket,
@@ -61,6 +61,8 @@ Layout make_layout(uint64_t nA, uint64_t nB, uint64_t S) {
     o = align_up(o + (L.nTiles + 1) * 8, 256);
     L.off_split_b = o;
     o = align_up(o + (L.nTiles + 1) * 8, 256);
+    L.off_samples = o;
+    o += pivot_samples_bytes(nA, nB, S);
     L.total = o;
     return L;
 }
@@ -620,8 +622,10 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
     uint64_t* status = reinterpret_cast<uint64_t*>(w + L.off_status);
     // the split kernel also clears the header, the partial counts and the
     // tiles' look-back status words
-    const si_status sst = pivot_split(dA, nA, dB, nB, kS, split_a, split_b, reinterpret_cast<uint64_t*>(w),
-                                      L.off_split_a / 8, d_count, stream);
+    uint32_t* samples_a = reinterpret_cast<uint32_t*>(w + L.off_samples);
+    uint32_t* samples_b = samples_a + align_up(((nA + kS - 1) / kS) * 4, 256) / 4;
+    const si_status sst = pivot_split(dA, nA, dB, nB, kS, split_a, split_b, samples_a, samples_b,
+                                      reinterpret_cast<uint64_t*>(w), L.off_split_a / 8, d_count, stream);
     if (sst != SI_OK) return sst;
 
     const uint64_t nGroups = (L.nTiles + kGroup - 1) / kGroup;

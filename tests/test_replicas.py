@@ -99,8 +99,8 @@ def test_reference_arm_ranks_above_zero_do_no_work(monkeypatch):
     import bench
 
     called = []
-    monkeypatch.setattr(bench, "cpu_measure", lambda *a, **k: called.append(a))
-    monkeypatch.setattr(bench, "sample_pair", lambda *a, **k: called.append(a))
+    monkeypatch.setattr(bench, "ref_sisi_measure", lambda *a, **k: called.append(a))
+    monkeypatch.setattr(bench, "ref_pair", lambda *a, **k: called.append(a))
 
     class Args:
         workload, steps, warmup, gpus = "sisi_large", 3, 3, 2
