@@ -191,38 +191,74 @@ constexpr uint32_t kWin = 16384;                // values per window
 constexpr uint32_t kWinWords = kWin / 32;       // 512 words: a 2 KiB bitmap per set
 constexpr int kStWarps = 8;                     // warps per CTA
 constexpr int kStBlock = kStWarps * 32;
-constexpr int kStCtasPerSm = 4;                 // 32 warps per SM
-constexpr uint32_t kChunk = 128;                // elements per chunk: one 16-byte group per lane
+constexpr int kStCtasPerSm = 3;                 // 24 warps per SM (85 registers each)
+constexpr uint32_t kChunk = 256;                // elements per chunk: two 16-byte groups per lane
 constexpr uint64_t kMinRange = 4096;            // X elements per warp, at least
-constexpr uint64_t kMaxStream = (1ull << 32) - 1024;  // stream positions (and 3 chunks ahead) are 32-bit
+constexpr uint64_t kMaxStream = (1ull << 32) - 1024;  // stream positions (and 2 chunks ahead) are 32-bit
 constexpr size_t kStSmem = size_t(kStWarps) * 2 * kWinWords * sizeof(uint32_t);  // 32 KiB
 
-// One sorted set read by a warp as chunks of 128 elements: lane l holds the
-// 16-byte group at position pc + 4 l of a 16-byte aligned base (element i0 of
-// the set sits at position v0 < 4); the next two chunks are loaded ahead.
-// Only positions [v0, v1) are elements, and a group is loaded only if it holds
-// one of them.  Positions are 32-bit: a stream is shorter than 2^32 - 4.
+// One sorted set read by a warp as chunks of 256 elements: lane l holds the
+// 16-byte groups at positions pc + 4 l and pc + 128 + 4 l of a 16-byte aligned
+// base; the next chunk is loaded ahead, and the one after it is prefetched
+// into L2.  The elements of the stream are positions [v0, v1) (v0 < 4); a group
+// is loaded only if it holds one of them.  Positions before v0 in the first
+// chunk hold a copy of the first element, positions from v1 on in the last
+// chunk a copy of the last, so every position of a chunk is an element of the
+// set (setting a bit twice is harmless) and nothing checks positions.
+// Positions are 32-bit: a stream is shorter than 2^32 - 1024.
 struct SetStream {
     const uint32_t* base;
-    uint32_t v0, v1, pc;
-    uint4 c, n1, n2;
+    uint32_t v1, pc;
+    uint4 c0, c1, n0, n1;
     uint32_t last;  // the current chunk's last element (its largest, in a sorted set)
 };
 
-__device__ __forceinline__ uint4 ld_stream(const uint32_t* base, uint32_t p, uint32_t v1) {
-    return p < v1 ? __ldcs(reinterpret_cast<const uint4*>(base + p)) : make_uint4(0u, 0u, 0u, 0u);
+// Loads the group at position p when p < v1 (streaming, evict-first);
+// otherwise g keeps its contents.
+__device__ __forceinline__ void ld_group(uint4& g, const uint32_t* base, uint32_t p, uint32_t v1) {
+    asm("{\n\t.reg .pred q;\n\t"
+        "setp.lt.u32 q, %4, %5;\n\t"
+        "@q ld.global.cs.v4.u32 {%0, %1, %2, %3}, [%6];\n\t}"
+        : "+r"(g.x), "+r"(g.y), "+r"(g.z), "+r"(g.w)
+        : "r"(p), "r"(v1), "l"(base + p));
 }
 
 __device__ __forceinline__ uint32_t comp(const uint4& v, uint32_t q) {
     return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
 }
 
-__device__ __forceinline__ void stream_last(SetStream& s) {
+__device__ __forceinline__ void set_comp(uint4& v, uint32_t q, uint32_t x) {
+    v.x = q == 0 ? x : v.x;
+    v.y = q == 1 ? x : v.y;
+    v.z = q == 2 ? x : v.z;
+    v.w = q == 3 ? x : v.w;
+}
+
+// Lane 0 asks the bulk-copy engine to bring the chunk at position p (the part
+// that holds elements) into L2; one predicated instruction, no branch.
+__device__ __forceinline__ void prefetch_chunk_l2(const SetStream& s, uint32_t p, uint32_t lead) {
+    const uint32_t bytes = (min(p + kChunk, (s.v1 + 3) & ~3u) - p) * 4;
+    asm volatile("{\n\t.reg .pred l, q;\n\t"
+                 "setp.ne.u32 l, %3, 0;\n\t"
+                 "setp.lt.and.u32 q, %0, %1, l;\n\t"
+                 "@q cp.async.bulk.prefetch.L2.global [%2], %4;\n\t}" ::"r"(p),
+                 "r"(s.v1), "l"(s.base + p), "r"(lead), "r"(bytes)
+                 : "memory");
+}
+
+// The current chunk's last element; in the stream's last chunk the positions
+// from v1 on get copies of it.
+__device__ __forceinline__ void stream_settle(SetStream& s, uint32_t lane) {
     if (s.pc + kChunk <= s.v1) {
-        s.last = __shfl_sync(kFullMask, s.c.w, 31);
-    } else {
-        const uint32_t lp = s.v1 - 1 - s.pc;  // < 128
-        s.last = __shfl_sync(kFullMask, comp(s.c, lp & 3), lp >> 2);
+        s.last = __shfl_sync(kFullMask, s.c1.w, 31);
+        return;
+    }
+    const uint32_t lp = s.v1 - 1 - s.pc;  // < 256
+    s.last = __shfl_sync(kFullMask, comp(lp >= 128 ? s.c1 : s.c0, lp & 3), (lp & 127) >> 2);
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+        if (s.pc + 4 * lane + q >= s.v1) set_comp(s.c0, q, s.last);
+        if (s.pc + 128 + 4 * lane + q >= s.v1) set_comp(s.c1, q, s.last);
     }
 }
 
@@ -230,49 +266,81 @@ __device__ __forceinline__ void stream_init(SetStream& s, const uint32_t* set, u
                                             uint32_t lane) {
     const uint64_t p0 = i0 + ((reinterpret_cast<uintptr_t>(set) & 15u) >> 2);  // from the aligned base below set
     s.base = set - (p0 - i0) + (p0 & ~uint64_t(3));
-    s.v0 = static_cast<uint32_t>(p0 & 3);
-    s.v1 = static_cast<uint32_t>(s.v0 + (i1 - i0));
+    const uint32_t v0 = static_cast<uint32_t>(p0 & 3);
+    s.v1 = static_cast<uint32_t>(v0 + (i1 - i0));
     s.pc = 0;
-    s.c = ld_stream(s.base, 4 * lane, s.v1);
-    s.n1 = ld_stream(s.base, kChunk + 4 * lane, s.v1);
-    s.n2 = ld_stream(s.base, 2 * kChunk + 4 * lane, s.v1);
+    s.c0 = s.c1 = s.n0 = s.n1 = make_uint4(0u, 0u, 0u, 0u);
+    ld_group(s.c0, s.base, 4 * lane, s.v1);
+    ld_group(s.c1, s.base, 128 + 4 * lane, s.v1);
+    ld_group(s.n0, s.base, kChunk + 4 * lane, s.v1);
+    ld_group(s.n1, s.base, kChunk + 128 + 4 * lane, s.v1);
+    prefetch_chunk_l2(s, 2 * kChunk, lane == 0);
+    prefetch_chunk_l2(s, 3 * kChunk, lane == 0);
+    // the first chunk: positions before v0 get copies of the first element
+    const uint32_t first = __shfl_sync(kFullMask, comp(s.c0, v0), 0);
+    if (lane == 0) {
+#pragma unroll
+        for (uint32_t q = 0; q < 3; ++q)
+            if (q < v0) set_comp(s.c0, q, first);
+    }
 }
 
-// Moves to the next chunk (false: there is none) and loads the one two ahead.
+// Moves to the next chunk (false: there is none), loads the one after it and
+// prefetches the one after that into L2.
 __device__ __forceinline__ bool stream_advance(SetStream& s, uint32_t lane) {
     if (s.pc + kChunk >= s.v1) return false;
     s.pc += kChunk;
-    s.c = s.n1;
-    s.n1 = s.n2;
-    s.n2 = ld_stream(s.base, s.pc + 2 * kChunk + 4 * lane, s.v1);
-    stream_last(s);
+    s.c0 = s.n0;
+    s.c1 = s.n1;
+    ld_group(s.n0, s.base, s.pc + kChunk + 4 * lane, s.v1);
+    ld_group(s.n1, s.base, s.pc + kChunk + 128 + 4 * lane, s.v1);
+    prefetch_chunk_l2(s, s.pc + 3 * kChunk, lane == 0);
+    stream_settle(s, lane);
     return true;
+}
+
+__device__ __forceinline__ void bit_or(uint32_t bm, uint32_t o) {
+    // ordered before the AND pass's loads by the __syncwarp between them
+    asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(bm + ((o >> 5) << 2)), "r"(__funnelshift_l(0u, 1u, o)));
 }
 
 // Sets the bits of the current chunk's elements v with a <= v < a + lim
 // (lim = kWin, or 2^32 - a for the top window, so that no smaller value
-// wraps into it).
-__device__ __forceinline__ void stream_insert(const SetStream& s, uint32_t* bm, uint32_t a, uint32_t lim,
-                                              uint32_t lane) {
-    const bool interior = s.pc >= s.v0 && s.pc + kChunk <= s.v1;
-    const uint32_t p = s.pc + 4 * lane;
+// wraps into it).  bm: shared-window address of the bitmap.
+__device__ __forceinline__ void stream_insert(const SetStream& s, uint32_t bm, uint32_t a, uint32_t lim) {
+    const uint32_t first = __shfl_sync(kFullMask, s.c0.x, 0);
+    if (first >= a && s.last - a < lim) {  // the whole chunk lies in the window
 #pragma unroll
-    for (uint32_t q = 0; q < 4; ++q) {
-        const uint32_t o = comp(s.c, q) - a;
-        const bool ok = o < lim && (interior || (p + q >= s.v0 && p + q < s.v1));
-        if (ok) atomicOr(bm + (o >> 5), __funnelshift_l(0u, 1u, o));
+        for (uint32_t h = 0; h < 2; ++h) {
+            const uint4& g = h ? s.c1 : s.c0;
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q) bit_or(bm, comp(g, q) - a);
+        }
+    } else {
+#pragma unroll
+        for (uint32_t h = 0; h < 2; ++h) {
+            const uint4& g = h ? s.c1 : s.c0;
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q) {
+                const uint32_t o = comp(g, q) - a;
+                if (o < lim) bit_or(bm, o);
+            }
+        }
     }
 }
 
 // The smallest element of the current chunk that is >= e (the chunk's last
 // element is >= e).
-__device__ __forceinline__ uint32_t stream_first_from(const SetStream& s, uint64_t e, uint32_t lane) {
+__device__ __forceinline__ uint32_t stream_first_from(const SetStream& s, uint64_t e) {
     uint32_t m = 0xffffffffu;
-    const uint32_t p = s.pc + 4 * lane;
 #pragma unroll
-    for (uint32_t q = 0; q < 4; ++q) {
-        const uint32_t v = comp(s.c, q);
-        if (p + q >= s.v0 && p + q < s.v1 && v >= e) m = min(m, v);
+    for (uint32_t h = 0; h < 2; ++h) {
+        const uint4& g = h ? s.c1 : s.c0;
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+            const uint32_t v = comp(g, q);
+            m = v >= e ? min(m, v) : m;
+        }
     }
     return __reduce_min_sync(kFullMask, m);
 }
@@ -294,6 +362,7 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t* bmx = smem + warp * 2 * kWinWords;
     uint32_t* bmy = bmx + kWinWords;
+    const uint32_t sbx = smem_addr(bmx), sby = smem_addr(bmy);
     uint4* bx4 = reinterpret_cast<uint4*>(bmx);
     uint4* by4 = reinterpret_cast<uint4*>(bmy);
     for (uint32_t i = lane; i < kWinWords / 2; i += 32) bx4[i] = make_uint4(0u, 0u, 0u, 0u);  // both bitmaps
@@ -309,8 +378,8 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
         uint64_t hits = 0;
         if (ys < nY) {
             stream_init(sy, Y, ys, nY, lane);
-            stream_last(sx);
-            stream_last(sy);
+            stream_settle(sx, lane);
+            stream_settle(sy, lane);
             uint32_t a = __ldg(Y + ys);  // >= vfirst: no X element below it can match
             uint32_t* dst = kOut ? scratch + ys : nullptr;
             for (;;) {
@@ -318,7 +387,7 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
                 const uint32_t lim = e > 0xffffffffull ? static_cast<uint32_t>(0x100000000ull - a) : kWin;
                 bool done = false;
                 for (;;) {
-                    stream_insert(sx, bmx, a, lim, lane);
+                    stream_insert(sx, sbx, a, lim);
                     if (sx.last >= e) break;
                     if (!stream_advance(sx, lane)) {
                         done = true;
@@ -326,7 +395,7 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
                     }
                 }
                 for (;;) {
-                    stream_insert(sy, bmy, a, lim, lane);
+                    stream_insert(sy, sby, a, lim);
                     if (sy.last >= e) break;
                     if (!stream_advance(sy, lane)) {
                         done = true;
@@ -359,7 +428,7 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
                 }
                 __syncwarp();
                 if (done) break;
-                const uint32_t fx = stream_first_from(sx, e, lane), fy = stream_first_from(sy, e, lane);
+                const uint32_t fx = stream_first_from(sx, e), fy = stream_first_from(sy, e);
                 a = max(fx, fy);
             }
         }
