@@ -199,28 +199,25 @@ constexpr size_t kStSmem = size_t(kStWarps) * 2 * kWinWords * sizeof(uint32_t); 
 
 // One sorted set read by a warp as chunks of 256 elements: lane l holds the
 // 16-byte groups at positions pc + 4 l and pc + 128 + 4 l of a 16-byte aligned
-// base; the next chunk is loaded ahead, and the one after it is prefetched
-// into L2.  The elements of the stream are positions [v0, v1) (v0 < 4); a group
-// is loaded only if it holds one of them.  Positions before v0 in the first
-// chunk hold a copy of the first element, positions from v1 on in the last
-// chunk a copy of the last, so every position of a chunk is an element of the
-// set (setting a bit twice is harmless) and nothing checks positions.
+// base.  Two register buffers alternate (ph = 0: the current chunk is in a,
+// the next one in b), so moving on copies nothing; the chunks four to eight
+// ahead are prefetched into L2 every fourth chunk.  The elements of the stream
+// are positions [v0, v1) (v0 < 4).  Positions before v0 in the first chunk hold
+// a copy of the first element, and positions from v1 on in the last chunk a
+// copy of the last, so every position of a chunk is an element of the set
+// (setting a bit twice is harmless) and nothing checks positions.  Loads past
+// the last group read the last group again (always a valid address).
 // Positions are 32-bit: a stream is shorter than 2^32 - 1024.
 struct SetStream {
     const uint32_t* base;
-    uint32_t v1, pc;
-    uint4 c0, c1, n0, n1;
+    uint32_t v1, pc, ph;
+    uint4 a0, a1, b0, b1;
     uint32_t last;  // the current chunk's last element (its largest, in a sorted set)
 };
 
-// Loads the group at position p when p < v1 (streaming, evict-first);
-// otherwise g keeps its contents.
-__device__ __forceinline__ void ld_group(uint4& g, const uint32_t* base, uint32_t p, uint32_t v1) {
-    asm("{\n\t.reg .pred q;\n\t"
-        "setp.lt.u32 q, %4, %5;\n\t"
-        "@q ld.global.cs.v4.u32 {%0, %1, %2, %3}, [%6];\n\t}"
-        : "+r"(g.x), "+r"(g.y), "+r"(g.z), "+r"(g.w)
-        : "r"(p), "r"(v1), "l"(base + p));
+__device__ __forceinline__ uint4 ld_group(const SetStream& s, uint32_t p) {
+    const uint32_t pend = (s.v1 - 1) & ~3u;  // the last group that holds elements
+    return __ldcs(reinterpret_cast<const uint4*>(s.base + min(p, pend)));
 }
 
 __device__ __forceinline__ uint32_t comp(const uint4& v, uint32_t q) {
@@ -234,10 +231,10 @@ __device__ __forceinline__ void set_comp(uint4& v, uint32_t q, uint32_t x) {
     v.w = q == 3 ? x : v.w;
 }
 
-// Lane 0 asks the bulk-copy engine to bring the chunk at position p (the part
-// that holds elements) into L2; one predicated instruction, no branch.
-__device__ __forceinline__ void prefetch_chunk_l2(const SetStream& s, uint32_t p, uint32_t lead) {
-    const uint32_t bytes = (min(p + kChunk, (s.v1 + 3) & ~3u) - p) * 4;
+// Lane 0 asks the bulk-copy engine to bring chunks [p, p + 4) (the part that
+// holds elements) into L2; one predicated instruction, no branch.
+__device__ __forceinline__ void prefetch_l2(const SetStream& s, uint32_t p, uint32_t lead) {
+    const uint32_t bytes = (min(p + 4 * kChunk, (s.v1 + 3) & ~3u) - p) * 4;
     asm volatile("{\n\t.reg .pred l, q;\n\t"
                  "setp.ne.u32 l, %3, 0;\n\t"
                  "setp.lt.and.u32 q, %0, %1, l;\n\t"
@@ -246,20 +243,18 @@ __device__ __forceinline__ void prefetch_chunk_l2(const SetStream& s, uint32_t p
                  : "memory");
 }
 
-// The current chunk's last element; in the stream's last chunk the positions
-// from v1 on get copies of it.
-__device__ __forceinline__ void stream_settle(SetStream& s, uint32_t lane) {
-    if (s.pc + kChunk <= s.v1) {
-        s.last = __shfl_sync(kFullMask, s.c1.w, 31);
-        return;
-    }
-    const uint32_t lp = s.v1 - 1 - s.pc;  // < 256
-    s.last = __shfl_sync(kFullMask, comp(lp >= 128 ? s.c1 : s.c0, lp & 3), (lp & 127) >> 2);
+// The last element of the chunk at pc held in (g0, g1); in the stream's last
+// chunk the positions from v1 on get copies of it.
+__device__ __forceinline__ uint32_t chunk_settle(uint4& g0, uint4& g1, uint32_t pc, uint32_t v1, uint32_t lane) {
+    if (pc + kChunk <= v1) return __shfl_sync(kFullMask, g1.w, 31);
+    const uint32_t lp = v1 - 1 - pc;  // < 256
+    const uint32_t last = __shfl_sync(kFullMask, comp(lp >= 128 ? g1 : g0, lp & 3), (lp & 127) >> 2);
 #pragma unroll
     for (uint32_t q = 0; q < 4; ++q) {
-        if (s.pc + 4 * lane + q >= s.v1) set_comp(s.c0, q, s.last);
-        if (s.pc + 128 + 4 * lane + q >= s.v1) set_comp(s.c1, q, s.last);
+        if (pc + 4 * lane + q >= v1) set_comp(g0, q, last);
+        if (pc + 128 + 4 * lane + q >= v1) set_comp(g1, q, last);
     }
+    return last;
 }
 
 __device__ __forceinline__ void stream_init(SetStream& s, const uint32_t* set, uint64_t i0, uint64_t i1,
@@ -269,33 +264,39 @@ __device__ __forceinline__ void stream_init(SetStream& s, const uint32_t* set, u
     const uint32_t v0 = static_cast<uint32_t>(p0 & 3);
     s.v1 = static_cast<uint32_t>(v0 + (i1 - i0));
     s.pc = 0;
-    s.c0 = s.c1 = s.n0 = s.n1 = make_uint4(0u, 0u, 0u, 0u);
-    ld_group(s.c0, s.base, 4 * lane, s.v1);
-    ld_group(s.c1, s.base, 128 + 4 * lane, s.v1);
-    ld_group(s.n0, s.base, kChunk + 4 * lane, s.v1);
-    ld_group(s.n1, s.base, kChunk + 128 + 4 * lane, s.v1);
-    prefetch_chunk_l2(s, 2 * kChunk, lane == 0);
-    prefetch_chunk_l2(s, 3 * kChunk, lane == 0);
+    s.ph = 0;
+    s.a0 = ld_group(s, 4 * lane);
+    s.a1 = ld_group(s, 128 + 4 * lane);
+    s.b0 = ld_group(s, kChunk + 4 * lane);
+    s.b1 = ld_group(s, kChunk + 128 + 4 * lane);
+    prefetch_l2(s, 2 * kChunk, lane == 0);
     // the first chunk: positions before v0 get copies of the first element
-    const uint32_t first = __shfl_sync(kFullMask, comp(s.c0, v0), 0);
+    const uint32_t first = __shfl_sync(kFullMask, comp(s.a0, v0), 0);
     if (lane == 0) {
 #pragma unroll
         for (uint32_t q = 0; q < 3; ++q)
-            if (q < v0) set_comp(s.c0, q, first);
+            if (q < v0) set_comp(s.a0, q, first);
     }
+    s.last = chunk_settle(s.a0, s.a1, 0, s.v1, lane);
 }
 
-// Moves to the next chunk (false: there is none), loads the one after it and
-// prefetches the one after that into L2.
+// Moves to the next chunk (false: there is none); the buffer it leaves takes
+// the chunk after that.
 __device__ __forceinline__ bool stream_advance(SetStream& s, uint32_t lane) {
     if (s.pc + kChunk >= s.v1) return false;
     s.pc += kChunk;
-    s.c0 = s.n0;
-    s.c1 = s.n1;
-    ld_group(s.n0, s.base, s.pc + kChunk + 4 * lane, s.v1);
-    ld_group(s.n1, s.base, s.pc + kChunk + 128 + 4 * lane, s.v1);
-    prefetch_chunk_l2(s, s.pc + 3 * kChunk, lane == 0);
-    stream_settle(s, lane);
+    const uint32_t p = s.pc + kChunk + 4 * lane;
+    if (s.ph == 0) {
+        s.a0 = ld_group(s, p);
+        s.a1 = ld_group(s, p + 128);
+        s.last = chunk_settle(s.b0, s.b1, s.pc, s.v1, lane);
+    } else {
+        s.b0 = ld_group(s, p);
+        s.b1 = ld_group(s, p + 128);
+        s.last = chunk_settle(s.a0, s.a1, s.pc, s.v1, lane);
+    }
+    s.ph ^= 1u;
+    if (((s.pc / kChunk) & 3) == 2) prefetch_l2(s, s.pc + 4 * kChunk, lane == 0);
     return true;
 }
 
@@ -304,45 +305,54 @@ __device__ __forceinline__ void bit_or(uint32_t bm, uint32_t o) {
     asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(bm + ((o >> 5) << 2)), "r"(__funnelshift_l(0u, 1u, o)));
 }
 
-// Sets the bits of the current chunk's elements v with a <= v < a + lim
-// (lim = kWin, or 2^32 - a for the top window, so that no smaller value
-// wraps into it).  bm: shared-window address of the bitmap.
-__device__ __forceinline__ void stream_insert(const SetStream& s, uint32_t bm, uint32_t a, uint32_t lim) {
-    const uint32_t first = __shfl_sync(kFullMask, s.c0.x, 0);
-    if (first >= a && s.last - a < lim) {  // the whole chunk lies in the window
+// Sets the bits of the chunk's elements v with a <= v < a + lim (lim = kWin,
+// or 2^32 - a for the top window, so that no smaller value wraps into it).
+// bm: shared-window address of the bitmap.
+__device__ __forceinline__ void chunk_insert(const uint4& g0, const uint4& g1, uint32_t last, uint32_t bm,
+                                             uint32_t a, uint32_t lim) {
+    if (__all_sync(kFullMask, g0.x >= a && last - a < lim)) {  // the whole chunk lies in the window
 #pragma unroll
-        for (uint32_t h = 0; h < 2; ++h) {
-            const uint4& g = h ? s.c1 : s.c0;
+        for (uint32_t q = 0; q < 4; ++q) bit_or(bm, comp(g0, q) - a);
 #pragma unroll
-            for (uint32_t q = 0; q < 4; ++q) bit_or(bm, comp(g, q) - a);
-        }
+        for (uint32_t q = 0; q < 4; ++q) bit_or(bm, comp(g1, q) - a);
     } else {
 #pragma unroll
-        for (uint32_t h = 0; h < 2; ++h) {
-            const uint4& g = h ? s.c1 : s.c0;
-#pragma unroll
-            for (uint32_t q = 0; q < 4; ++q) {
-                const uint32_t o = comp(g, q) - a;
-                if (o < lim) bit_or(bm, o);
-            }
+        for (uint32_t q = 0; q < 4; ++q) {
+            const uint32_t o0 = comp(g0, q) - a, o1 = comp(g1, q) - a;
+            if (o0 < lim) bit_or(bm, o0);
+            if (o1 < lim) bit_or(bm, o1);
         }
+    }
+}
+
+// Inserts the stream's chunks into the bitmap until one reaches past e (it
+// stays current: its later elements belong to later windows); false when the
+// stream ran out.
+__device__ __forceinline__ bool stream_fill(SetStream& s, uint32_t bm, uint32_t a, uint32_t lim, uint64_t e,
+                                            uint32_t lane) {
+    for (;;) {
+        if (s.ph == 0) chunk_insert(s.a0, s.a1, s.last, bm, a, lim);
+        else chunk_insert(s.b0, s.b1, s.last, bm, a, lim);
+        if (__all_sync(kFullMask, s.last >= e)) return true;
+        if (!stream_advance(s, lane)) return false;
     }
 }
 
 // The smallest element of the current chunk that is >= e (the chunk's last
 // element is >= e).
-__device__ __forceinline__ uint32_t stream_first_from(const SetStream& s, uint64_t e) {
+__device__ __forceinline__ uint32_t chunk_first_from(const uint4& g0, const uint4& g1, uint64_t e) {
     uint32_t m = 0xffffffffu;
 #pragma unroll
-    for (uint32_t h = 0; h < 2; ++h) {
-        const uint4& g = h ? s.c1 : s.c0;
-#pragma unroll
-        for (uint32_t q = 0; q < 4; ++q) {
-            const uint32_t v = comp(g, q);
-            m = v >= e ? min(m, v) : m;
-        }
+    for (uint32_t q = 0; q < 4; ++q) {
+        const uint32_t v0 = comp(g0, q), v1 = comp(g1, q);
+        m = v0 >= e ? min(m, v0) : m;
+        m = v1 >= e ? min(m, v1) : m;
     }
     return __reduce_min_sync(kFullMask, m);
+}
+
+__device__ __forceinline__ uint32_t stream_first_from(const SetStream& s, uint64_t e) {
+    return s.ph == 0 ? chunk_first_from(s.a0, s.a1, e) : chunk_first_from(s.b0, s.b1, e);
 }
 
 // One warp per range r of X: X elements [r L, (r + 1) L) and the Y elements
@@ -372,36 +382,19 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
     for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * kStWarps + warp; r < nRanges; r += nwarps) {
         const uint64_t xs = r * L, xe = min(xs + L, nX);
         SetStream sx, sy;
-        stream_init(sx, X, xs, xe, lane);  // loads in flight during the search below
+        stream_init(sx, X, xs, xe, lane);
         const uint32_t vfirst = __ldg(X + xs);
         const uint64_t ys = warp_first_true(0, nY, [&](uint64_t i) { return __ldg(Y + i) >= vfirst; });
-        uint64_t hits = 0;
+        uint32_t hits = 0;
         if (ys < nY) {
             stream_init(sy, Y, ys, nY, lane);
-            stream_settle(sx, lane);
-            stream_settle(sy, lane);
             uint32_t a = __ldg(Y + ys);  // >= vfirst: no X element below it can match
             uint32_t* dst = kOut ? scratch + ys : nullptr;
             for (;;) {
                 const uint64_t e = static_cast<uint64_t>(a) + kWin;
                 const uint32_t lim = e > 0xffffffffull ? static_cast<uint32_t>(0x100000000ull - a) : kWin;
-                bool done = false;
-                for (;;) {
-                    stream_insert(sx, sbx, a, lim);
-                    if (sx.last >= e) break;
-                    if (!stream_advance(sx, lane)) {
-                        done = true;
-                        break;
-                    }
-                }
-                for (;;) {
-                    stream_insert(sy, sby, a, lim);
-                    if (sy.last >= e) break;
-                    if (!stream_advance(sy, lane)) {
-                        done = true;
-                        break;
-                    }
-                }
+                const bool more_x = stream_fill(sx, sbx, a, lim, e, lane);
+                const bool more_y = stream_fill(sy, sby, a, lim, e, lane);
                 __syncwarp();
                 // AND of the window's bitmaps, a quarter (128 words) at a
                 // time, lane l holding words 4 l .. 4 l + 3 of the quarter
@@ -411,15 +404,16 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
                     const uint4 p = bx4[i], q = by4[i];
                     bx4[i] = make_uint4(0u, 0u, 0u, 0u);
                     by4[i] = make_uint4(0u, 0u, 0u, 0u);
-                    uint32_t m[4] = {p.x & q.x, p.y & q.y, p.z & q.z, p.w & q.w};
+                    const uint32_t m[4] = {p.x & q.x, p.y & q.y, p.z & q.z, p.w & q.w};
                     const uint32_t c = __popc(m[0]) + __popc(m[1]) + __popc(m[2]) + __popc(m[3]);
                     if constexpr (kOut) {
+                        // this lane's hits go to dst[hits + (hits of the lanes before it) ...]
                         const uint32_t incl = warp_inclusive_scan(c);
-                        uint64_t pos = hits + incl - c;
+                        uint32_t* o = dst + (hits + incl - c);
                         const uint32_t wbase = a + 32 * 4 * i;
 #pragma unroll
                         for (uint32_t j = 0; j < 4; ++j) {
-                            for (uint32_t mm = m[j]; mm; mm &= mm - 1) dst[pos++] = wbase + 32 * j + (__ffs(mm) - 1);
+                            for (uint32_t mm = m[j]; mm; mm &= mm - 1) *o++ = wbase + 32 * j + (__ffs(mm) - 1);
                         }
                         hits += __shfl_sync(kFullMask, incl, 31);
                     } else {
@@ -427,14 +421,13 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
                     }
                 }
                 __syncwarp();
-                if (done) break;
-                const uint32_t fx = stream_first_from(sx, e), fy = stream_first_from(sy, e);
-                a = max(fx, fy);
+                if (!more_x || !more_y) break;
+                a = max(stream_first_from(sx, e), stream_first_from(sy, e));
             }
         }
         if constexpr (kOut) {
             if (lane == 0) {
-                range_count[r] = static_cast<uint32_t>(hits);
+                range_count[r] = hits;
                 range_y[r] = ys < nY ? ys : nY;
             }
         } else {
