@@ -195,7 +195,7 @@ constexpr int kStCtasPerSm = 3;                 // 24 warps per SM (85 registers
 constexpr uint32_t kChunk = 256;                // elements per chunk: two 16-byte groups per lane
 constexpr uint64_t kMinRange = 4096;            // X elements per warp, at least
 constexpr uint64_t kMaxStream = (1ull << 32) - 1024;  // stream positions (and 2 chunks ahead) are 32-bit
-constexpr size_t kStSmem = size_t(kStWarps) * 2 * kWinWords * sizeof(uint32_t);  // 32 KiB
+constexpr size_t kStSmem = size_t(kStWarps) * 2 * kWinWords * sizeof(uint32_t) + 2048;  // 32 KiB, 2 KiB aligned
 
 // One sorted set read by a warp as chunks of 256 elements: lane l holds the
 // 16-byte groups at positions pc + 4 l and pc + 128 + 4 l of a 16-byte aligned
@@ -281,28 +281,33 @@ __device__ __forceinline__ void stream_init(SetStream& s, const uint32_t* set, u
 }
 
 // Moves to the next chunk (false: there is none); the buffer it leaves takes
-// the chunk after that.
+// the chunk after that.  kFromA: the current chunk is in a (ph == 0).
+template <bool kFromA>
 __device__ __forceinline__ bool stream_advance(SetStream& s, uint32_t lane) {
     if (s.pc + kChunk >= s.v1) return false;
     s.pc += kChunk;
     const uint32_t p = s.pc + kChunk + 4 * lane;
-    if (s.ph == 0) {
+    if constexpr (kFromA) {
         s.a0 = ld_group(s, p);
         s.a1 = ld_group(s, p + 128);
         s.last = chunk_settle(s.b0, s.b1, s.pc, s.v1, lane);
+        s.ph = 1;
     } else {
         s.b0 = ld_group(s, p);
         s.b1 = ld_group(s, p + 128);
         s.last = chunk_settle(s.a0, s.a1, s.pc, s.v1, lane);
+        s.ph = 0;
     }
-    s.ph ^= 1u;
     if (((s.pc / kChunk) & 3) == 2) prefetch_l2(s, s.pc + 4 * kChunk, lane == 0);
     return true;
 }
 
+// Sets bit o (< kWin) of the bitmap at shared-window address bm, which is
+// 2 KiB aligned: the word's address is one LOP3 of bm and o >> 3.
 __device__ __forceinline__ void bit_or(uint32_t bm, uint32_t o) {
     // ordered before the AND pass's loads by the __syncwarp between them
-    asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(bm + ((o >> 5) << 2)), "r"(__funnelshift_l(0u, 1u, o)));
+    asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(bm | ((o >> 3) & (4 * kWinWords - 4))),
+                 "r"(__funnelshift_l(0u, 1u, o)));
 }
 
 // Sets the bits of the chunk's elements v with a <= v < a + lim (lim = kWin,
@@ -330,11 +335,15 @@ __device__ __forceinline__ void chunk_insert(const uint4& g0, const uint4& g1, u
 // stream ran out.
 __device__ __forceinline__ bool stream_fill(SetStream& s, uint32_t bm, uint32_t a, uint32_t lim, uint64_t e,
                                             uint32_t lane) {
-    for (;;) {
-        if (s.ph == 0) chunk_insert(s.a0, s.a1, s.last, bm, a, lim);
-        else chunk_insert(s.b0, s.b1, s.last, bm, a, lim);
+    for (;;) {  // the buffers alternate: a, b, a, ...
+        if (s.ph == 0) {
+            chunk_insert(s.a0, s.a1, s.last, bm, a, lim);
+            if (__all_sync(kFullMask, s.last >= e)) return true;
+            if (!stream_advance<true>(s, lane)) return false;
+        }
+        chunk_insert(s.b0, s.b1, s.last, bm, a, lim);
         if (__all_sync(kFullMask, s.last >= e)) return true;
-        if (!stream_advance(s, lane)) return false;
+        if (!stream_advance<false>(s, lane)) return false;
     }
 }
 
@@ -370,7 +379,9 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
     uint32_t* __restrict__ scratch, uint64_t* __restrict__ d_count) {
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t* bmx = smem + warp * 2 * kWinWords;
+    // bitmaps 2 KiB aligned in the shared window (bit_or forms word addresses with one LOP3)
+    const uint32_t skew = ((smem_addr(smem) + 2047u) & ~2047u) - smem_addr(smem);
+    uint32_t* bmx = smem + skew / 4 + warp * 2 * kWinWords;
     uint32_t* bmy = bmx + kWinWords;
     const uint32_t sbx = smem_addr(bmx), sby = smem_addr(bmy);
     uint4* bx4 = reinterpret_cast<uint4*>(bmx);
