@@ -45,7 +45,6 @@
 // instead (binary search in shared memory); one with more than 512 Y elements
 // probes them from the ring.
 #include <algorithm>
-#include <cub/device/device_scan.cuh>
 
 #include "si_device.cuh"
 #include "si_internal.h"
@@ -376,7 +375,8 @@ template <bool kOut>
 __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
     const uint32_t* __restrict__ X, uint64_t nX, const uint32_t* __restrict__ Y, uint64_t nY, uint64_t L,
     uint64_t nRanges, uint32_t* __restrict__ range_count, uint64_t* __restrict__ range_y,
-    uint32_t* __restrict__ scratch, uint64_t* __restrict__ d_count) {
+    uint64_t* __restrict__ range_off, uint32_t* __restrict__ scratch, uint64_t* __restrict__ d_count,
+    uint32_t* __restrict__ done_ctas) {
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // bitmaps 2 KiB aligned in the shared window (bit_or forms word addresses with one LOP3)
@@ -447,6 +447,39 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
     }
     if constexpr (!kOut) {
         if (lane == 0 && my_hits) atomicAdd(reinterpret_cast<unsigned long long*>(d_count), my_hits);
+    } else {
+        // the last CTA to finish turns the ranges' counts into output offsets
+        __shared__ uint32_t s_last;
+        __shared__ uint64_t s_warp[kStWarps];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            s_last = atomicAdd(done_ctas, 1u) == gridDim.x - 1;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const uint64_t per = (nRanges + kStBlock - 1) / kStBlock;
+            const uint64_t r0 = nRanges < threadIdx.x * per ? nRanges : threadIdx.x * per;
+            const uint64_t r1 = nRanges < r0 + per ? nRanges : r0 + per;
+            uint64_t sum = 0;
+            for (uint64_t r = r0; r < r1; ++r) sum += __ldcg(range_count + r);
+            uint64_t incl = sum;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint64_t n = __shfl_up_sync(kFullMask, incl, d);
+                if (static_cast<int>(lane) >= d) incl += n;
+            }
+            if (lane == 31) s_warp[warp] = incl;
+            __syncthreads();
+            uint64_t before = 0;
+            for (uint32_t w = 0; w < warp; ++w) before += s_warp[w];
+            uint64_t off = before + incl - sum;
+            for (uint64_t r = r0; r < r1; ++r) {
+                range_off[r] = off;
+                off += __ldcg(range_count + r);
+            }
+        }
     }
 }
 
@@ -456,12 +489,13 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
 // next tile's count and offsets are loaded while the current one is copied,
 // and each lane keeps 8 loads in flight.  The warp of the last tile writes
 // the total count.
-constexpr int kCopyUnroll = 8;
+constexpr int kCopyUnroll = 16;
 __global__ void __launch_bounds__(256) bp_copy_kernel(const uint32_t* __restrict__ tile_count,
                                                       const uint64_t* __restrict__ tile_off,
                                                       const uint64_t* __restrict__ split_y, uint64_t nTiles,
                                                       const uint32_t* __restrict__ scratch, uint32_t* __restrict__ out,
                                                       uint64_t out_cap, uint64_t* __restrict__ d_count, uint32_t* err) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // the counts, offsets and hits of the tile kernel
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x / 32);
     uint64_t t = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
@@ -507,16 +541,16 @@ __global__ void __launch_bounds__(256) bp_copy_kernel(const uint32_t* __restrict
     if (overflow) record_error(err, SI_ERR_OUTPUT_OVERFLOW, 9, 0);
 }
 
-// Workspace of the bitmap stream: header (error word), per-range hit counts,
-// Y starts and output offsets, the scratch array of the hits (as long as Y)
-// and the scan's temporary storage.
+// Workspace of the bitmap stream: header (error word, finished-CTA counter),
+// per-range hit counts, Y starts and output offsets, and the scratch array of
+// the hits (as long as Y).
 constexpr size_t kHeaderBytes = 256;
+constexpr size_t kDoneCtas = 32;  // header word: CTAs of the stream kernel that finished
 constexpr uint64_t kRangesBasis = 148 * kStCtasPerSm * kStWarps;  // one range per resident warp of a B200
 
 struct BpLayout {
     uint64_t nRanges = 0, L = 0;
-    size_t off_count = 0, off_y = 0, off_off = 0, off_scratch = 0, off_cub = 0, cub_bytes = 0, total = 0,
-           total_count_only = 0;
+    size_t off_count = 0, off_y = 0, off_off = 0, off_scratch = 0, total = 0, total_count_only = 0;
 };
 
 BpLayout make_bp_layout(uint64_t nA, uint64_t nB) {
@@ -530,17 +564,7 @@ BpLayout make_bp_layout(uint64_t nA, uint64_t nB) {
     L.off_y = o;       o = align_up(o + L.nRanges * 8, 256);
     L.off_off = o;     o = align_up(o + L.nRanges * 8, 256);
     L.off_scratch = o; o = align_up(o + nY * 4, 256);
-    // without a device to ask, a bound of 1 MiB
-    size_t bytes = 0;
-    if (L.nRanges > 0x7fffffffull ||
-        cub::DeviceScan::ExclusiveScan(nullptr, bytes, static_cast<const uint32_t*>(nullptr),
-                                       static_cast<uint64_t*>(nullptr), cub::Sum(), uint64_t(0),
-                                       static_cast<int>(std::max<uint64_t>(1, L.nRanges))) != cudaSuccess)
-        bytes = 1u << 20;
-    cudaGetLastError();  // a failed query leaves no sticky error behind
-    L.cub_bytes = align_up(bytes, 256);
-    L.off_cub = o;
-    L.total = o + L.cub_bytes;
+    L.total = o;
     return L;
 }
 
@@ -616,29 +640,21 @@ si_status bm_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
         const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(
             (L.nRanges + kStWarps - 1) / kStWarps, static_cast<uint64_t>(sm_count()) * kStCtasPerSm));
         PhaseTimer timer("sisi_tile", stream);
-        kernel<<<grid, kStBlock, kStSmem, stream>>>(X, nX, Y, nY, L.L, L.nRanges, range_count, range_y, scratch,
-                                                    d_count);
+        kernel<<<grid, kStBlock, kStSmem, stream>>>(X, nX, Y, nY, L.L, L.nRanges, range_count, range_y, range_off,
+                                                    scratch, d_count, reinterpret_cast<uint32_t*>(w + kDoneCtas));
         SI_LAUNCH_CHECK("bp_stream_kernel");
         return SI_OK;
     };
     if (!d_out) return launch(bp_stream_kernel<false>);
     si_status st = launch(bp_stream_kernel<true>);
     if (st != SI_OK) return st;
-    {
-        PhaseTimer timer("sisi_scan", stream);
-        size_t bytes = L.cub_bytes;
-        SI_CUDA_TRY(cub::DeviceScan::ExclusiveScan(w + L.off_cub, bytes, range_count, range_off, cub::Sum(),
-                                                   uint64_t(0), static_cast<int>(L.nRanges), stream));
-    }
-    {
-        PhaseTimer timer("sisi_copy", stream);
-        const unsigned grid = static_cast<unsigned>(
-            std::max<uint64_t>(1, std::min<uint64_t>((L.nRanges + 7) / 8, static_cast<uint64_t>(sm_count()) * 8)));
-        bp_copy_kernel<<<grid, 256, 0, stream>>>(range_count, range_off, range_y, L.nRanges, scratch, d_out, out_cap,
-                                                 d_count, reinterpret_cast<uint32_t*>(w));
-        SI_LAUNCH_CHECK("bp_copy_kernel");
-    }
-    return SI_OK;
+    PhaseTimer timer("sisi_copy", stream);
+    const unsigned grid = static_cast<unsigned>(
+        std::max<uint64_t>(1, std::min<uint64_t>((L.nRanges + 7) / 8, static_cast<uint64_t>(sm_count()) * 8)));
+    return launch_dependent(bp_copy_kernel, dim3(grid), dim3(256), 0, stream,
+                            static_cast<const uint32_t*>(range_count), static_cast<const uint64_t*>(range_off),
+                            static_cast<const uint64_t*>(range_y), L.nRanges, static_cast<const uint32_t*>(scratch),
+                            d_out, out_cap, d_count, reinterpret_cast<uint32_t*>(w));
 }
 
 }  // namespace si
