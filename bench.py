@@ -25,7 +25,7 @@ Metric: Gelem/s = (|A| + |B|) / step time.
           count + elements D2H, per step, pipelined over 8 value ranges.
   roofline  live per-launch time of the dominant kernel (the tile kernel) from the
           library's phase timer over the timed region, against measured HBM;
-          phase_avg_ms lists every phase of the step (split, tiles, scan, copy).
+          phase_avg_ms lists every phase of the step (set-up, stream/tiles, copy).
   cpu_baseline  the reference's own CPU executable (oracle/_ref/stdintersection,
           built from the reference sources) on value-range slices of the same
           pair, timed by the reference's HostTimer.
@@ -97,15 +97,12 @@ def log(*a):
 SKEW_RATIO = 64  # SI_TECH_AUTO: obs when one set is more than this many times the other
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu
-# captures summarised in profiles/: the 2^25 x 2^25 captures of the ip tile
-# kernel (268.73 MB read + 13.22 MB written) and of the bitmap engine's
-# bm_stage_kernel (268.64 MB + 14.60 MB), scaled by 8 to the 2^28 x 2^28 launch
-# (tiles, inputs and matches all grow in proportion).
+# captures summarised in profiles/: the 2^25 x 2^25 captures (sisi_mid) of the
+# ip tile kernel and of the bitmap engine's bp_stream_kernel, scaled by 8 to
+# the 2^28 x 2^28 launch (ranges, inputs and matches all grow in proportion).
 TRAFFIC_PER_LAUNCH = {
     "ip/sisi_large/out": 8 * (268.727808e6 + 13.220096e6),
     "ip/sisi_mid/out": 268.727808e6 + 13.220096e6,
-    "bitmap/sisi_large/out": 8 * (268.642816e6 + 14.604288e6),
-    "bitmap/sisi_mid/out": 268.642816e6 + 14.604288e6,
 }
 
 
@@ -365,7 +362,7 @@ def run_ours(args, rank: int, world: int):
     tile_ms, tile_n = ctypes.c_double(0), ctypes.c_uint64(0)
     lib.si_timer_read(b"sisi_tile", ctypes.byref(tile_ms), ctypes.byref(tile_n))
     phases = {}
-    for ph in ("sisi_prepare", "sisi_split", "sisi_tile", "sisi_scan", "sisi_copy", "obs_sample", "obs_search",
+    for ph in ("sisi_split", "sisi_tile", "sisi_scan", "sisi_copy", "obs_sample", "obs_search",
                "obs_scan", "obs_compact"):
         p_ms, p_n = ctypes.c_double(0), ctypes.c_uint64(0)
         lib.si_timer_read(ph.encode(), ctypes.byref(p_ms), ctypes.byref(p_n))
@@ -423,7 +420,7 @@ def run_ours(args, rank: int, world: int):
     kernel, launches = {
         "ip": ("ip_tile_kernel<merge path>", 3),
         "hi": ("ip_tile_kernel<hash probe>", 3),
-        "bitmap": ("bm_stage_kernel", 7 if args.materialize else 3),
+        "bitmap": ("bp_stream_kernel", 2 if args.materialize else 1),
         "obs": ("obs_search_kernel", 4 if args.materialize else 2),
     }[engine]
     if engine == "obs":

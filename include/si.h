@@ -147,11 +147,17 @@ si_status si_sisi_host_ctx(si_host_ctx* ctx, const uint32_t* hA, uint64_t nA, co
  * SI_ERR_WORKSPACE_TOO_SMALL before anything is launched.  The first call on a
  * device looks up the array's device address (issue it before any stream
  * capture).  All calls share the array: calls that may overlap on the GPU
- * (e.g. on unordered streams) race and must not be issued.  Device-detected
- * input errors are not reported (there is no caller workspace to read);
- * check inputs with si_validate_sorted. */
+ * (e.g. on unordered streams) race and must not be issued.  A call returns
+ * only the host-side status; what its kernels record on the device (input
+ * that is not strictly increasing, a bounded wait that gave up) stays in the
+ * array's error word until the next call clears it: si_sisi_noalloc_check
+ * reads it. */
 si_status si_sisi_noalloc(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB,
                           uint64_t* d_count, uint32_t* d_out, uint64_t out_cap, si_stream_t stream);
+/* Synchronises the stream and returns the error that the last si_sisi_noalloc
+ * call on this device recorded on the device (SI_OK if none).  Allocates
+ * nothing.  No counterpart in the reference. */
+si_status si_sisi_noalloc_check(si_stream_t stream);
 
 /* Synchronises the stream and returns the error recorded in a workspace by the
  * last call that used it (SI_OK if none). */
@@ -160,6 +166,14 @@ si_status si_workspace_check(const void* d_workspace, si_stream_t stream);
 /* Same, plus where on the device the error was recorded (site: an id of the
  * bounded wait or check that gave up; detail: site-specific, e.g. a tile). */
 si_status si_workspace_diagnostic(const void* d_workspace, si_stream_t stream, uint32_t* site, uint32_t* detail);
+
+/* Self-test of the engine's bounded device waits (every wait of every kernel
+ * gives up after a time limit, records SI_ERR_TIMEOUT with a site id in the
+ * workspace's error word and lets its kernel end).  One thread waits on an
+ * mbarrier phase that nothing completes, for limit_ns (<= 4 s); synchronises
+ * the stream and returns the error word: SI_ERR_TIMEOUT when the wait gave up
+ * as it should.  d_workspace: >= 16 bytes, 16-byte aligned. */
+si_status si_wait_selftest(void* d_workspace, uint64_t limit_ns, si_stream_t stream);
 
 /* Device-side check that x[0..n) is strictly increasing.  Writes 1 (ok) or 0
  * to d_flag (device uint32).  No workspace. */

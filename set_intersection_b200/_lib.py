@@ -71,6 +71,7 @@ _SIGNATURES = {
     "si_sisi_workspace_size": (_sz, [_u64, _u64, _int]),
     "si_sisi": (_int, [_vp, _u64, _vp, _u64, _int, _vp, _vp, _u64, _vp, _sz, _vp]),
     "si_sisi_noalloc": (_int, [_vp, _u64, _vp, _u64, _vp, _vp, _u64, _vp]),
+    "si_sisi_noalloc_check": (_int, [_vp]),
     "si_sisi_host_workspace_size": (_sz, [_vp, _u64, _vp, _u64, _int, ctypes.c_uint32]),
     "si_sisi_host": (_int, [_vp, _u64, _vp, _u64, _int, ctypes.c_uint32, ctypes.POINTER(_u64), _vp, _u64, _vp, _sz,
                             _vp]),
@@ -81,6 +82,7 @@ _SIGNATURES = {
     "si_workspace_check": (_int, [_vp, _vp]),
     "si_workspace_diagnostic": (_int, [_vp, _vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     "si_validate_sorted": (_int, [_vp, _u64, _vp, _vp]),
+    "si_wait_selftest": (_int, [_vp, _u64, _vp]),
     "si_gen_uniform": (_int, [_u64, _u64, _u64, _u64, _vp, _int]),
     "si_gen_bernoulli": (_int, [_u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, _vp, _vp, _int]),
     "si_gen_powerlaw": (_int, [_u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,

@@ -88,6 +88,18 @@ __global__ void validate_sorted_kernel(const uint32_t* __restrict__ x, uint64_t 
 
 __global__ void set_flag_kernel(uint32_t* flag, uint32_t v) { *flag = v; }
 
+// One thread waits, with a time limit, on an mbarrier phase that nothing
+// completes: the wait must give up, record SI_ERR_TIMEOUT in the error word
+// and let the kernel end.
+__global__ void wait_selftest_kernel(uint32_t* err, uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    err[0] = err[1] = err[2] = err[3] = 0;
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_wait_bounded(&bar, 0, err, 31, 0, limit_ns);
+}
+
 bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
 
 }  // namespace
@@ -347,6 +359,15 @@ si_status si_workspace_diagnostic(const void* d_workspace, si_stream_t stream, u
     *site = words[1];
     *detail = words[2];
     return static_cast<si_status>(words[0]);
+}
+
+si_status si_wait_selftest(void* d_workspace, uint64_t limit_ns, si_stream_t stream) {
+    if (!d_workspace || !si::aligned(d_workspace, 16) || limit_ns == 0 || limit_ns > si::kWaitLimitNs)
+        return SI_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    si::wait_selftest_kernel<<<1, 32, 0, s>>>(static_cast<uint32_t*>(d_workspace), limit_ns);
+    SI_LAUNCH_CHECK("wait_selftest_kernel");
+    return si_workspace_check(d_workspace, stream);
 }
 
 si_status si_validate_sorted(const uint32_t* d_x, uint64_t n, uint32_t* d_flag, si_stream_t stream) {

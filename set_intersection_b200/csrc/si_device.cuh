@@ -22,15 +22,16 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Deadline helper for a bounded wait: expired() becomes true kWaitLimitNs
-// after construction.
+// Deadline helper for a bounded wait: expired() becomes true `limit_ns`
+// (default kWaitLimitNs) after construction.
 struct WaitBudget {
-    uint64_t start;
+    uint64_t start, limit;
     uint32_t polls = 0;
-    __device__ __forceinline__ WaitBudget() : start(global_ns()) {}
+    __device__ __forceinline__ explicit WaitBudget(uint64_t limit_ns = kWaitLimitNs)
+        : start(global_ns()), limit(limit_ns) {}
     __device__ __forceinline__ bool expired() {
         // the timer is read every 32 polls
-        return ((++polls & 31u) == 0) && (global_ns() - start > kWaitLimitNs);
+        return ((++polls & 31u) == 0) && (global_ns() - start > limit);
     }
 };
 
@@ -107,9 +108,9 @@ constexpr uint32_t kSuspendHintNs = 1u << 20;
 // Bounded wait on an mbarrier phase; records SI_ERR_TIMEOUT and returns false
 // if it gives up.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err, uint32_t site = 0,
-                                                  uint32_t info = 0) {
+                                                  uint32_t info = 0, uint64_t limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
-    WaitBudget budget;
+    WaitBudget budget(limit_ns);
     while (!budget.expired()) {
         if (mbar_try_wait_suspend(bar, parity, kSuspendHintNs)) return true;
     }
@@ -130,6 +131,21 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 // Named barrier over `count` threads (id 0 is __syncthreads).
 __device__ __forceinline__ void named_barrier(uint32_t id, uint32_t count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Named barrier that also ORs a predicate over the `count` threads: every
+// thread gets true if any passed true.
+__device__ __forceinline__ bool named_barrier_or(uint32_t id, uint32_t count, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "barrier.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(v ? 1u : 0u), "r"(id), "r"(count)
+        : "memory");
+    return r != 0;
 }
 
 __device__ __forceinline__ uint64_t ld_acquire_shared_u64(const uint64_t* p) {

@@ -1,49 +1,40 @@
 // si_sisi_bitmap.cu -- technique bitmap for one pair of large sorted sets
 // (and SI_TECH_AUTO for pairs of similar size), plus the value-pivot split
-// shared with the intersect-path tiles.
+// that the intersect-path tiles use.
 //
 // Replaces the single-instance path of bitmap_dynamic (src/bitmap_dynamic.cu:
 // 168-176: constructBitmap over the whole universe, singleInstanceIntersect,
 // thrust::reduce).  The reference sets one bit per element of A in a bitmap as
 // large as the universe (2^31 bits = 256 MiB for the 2^28 x 2^28 pair) and
 // probes it with every element of B from global memory.  Here the bitmaps are
-// small and private to a warp, and live in shared memory:
+// small, private to a warp and cover a window of 16384 values at a time:
 //
-//  K1  pivot_sample_kernel: every S-th element of each set (the pivots) into
-//      two compact sample arrays; clears the workspace header and the count.
-//  K2  pivot_split_kernel: one warp per pivot finds its rank in the merged
-//      pivot order (a merge-path search over the compact samples, which stay
-//      in L2) and its exact split in the other set: a 128-element probe at the
-//      position interpolated between the window's end samples, with a warp
-//      search of the window when the probe misses.  Consecutive pivots bound a
-//      tile to <= S elements of each set; a tile boundary is a value, so an
-//      equal pair is never split.
-//  K3  bp_tile_kernel, persistent, one CTA of 32 warps per SM:
-//        warp 30 lane 0  stages tiles (ticket order) into a 192 KiB shared ring
-//                        with bulk copies (TMA), several tiles ahead;
-//        warp 31         per staged tile, the Y start of every consumer's range
-//                        (a binary search per lane in the staged Y part);
-//        warps 0..29     consumer w takes the X elements [w nx/30, (w+1) nx/30)
-//                        of the tile and the Y elements of the same value range;
-//                        it loads its Y elements into registers, sets the bits
-//                        of its X elements in its own 1 KiB bitmap (values v0 ..
-//                        v0 + 8191, v0 its first X element), releases the ring
-//                        slot and probes the bitmap from the registers.
-//      Consumers never meet at a barrier.  With element output each one
-//      publishes its hit count in shared memory (tagged with the tile's
-//      sequence number), adds up the counts of the consumers before it in the
-//      same tile and writes its hits, in order, to scratch[first Y index of the
-//      tile + that prefix ...]; the last consumer writes the tile's count.
-//  K4  exclusive scan of the tile counts (CUB).
-//  K5  bp_copy_kernel: each tile's hits from scratch to out (a warp per tile)
-//      and the total count.
-// Count-only mode runs K1-K3 and adds the hits into d_count.
+//  bp_stream_kernel  one warp per range of the larger set X (ranges of equal
+//      element count, about one per resident warp), streaming X's range and the
+//      smaller set Y from the first element not below the range's start, both
+//      with coalesced 16-byte loads one chunk (256 elements) ahead and bulk L2
+//      prefetches four to eight chunks ahead.  Per window of values each
+//      stream's elements set bits in its own 2 KiB bitmap (shared red.or, no
+//      barrier: the warp owns its bitmaps); the AND of the two bitmaps is the
+//      window's part of the intersection, in value order.  The next window
+//      starts at the larger of the two sets' next elements, so stretches where
+//      one set has no element are skipped.  Counting: popcounts.  Element
+//      output: each warp writes its range's hits in order to a scratch array
+//      (at the range's first Y index) and their number; the last CTA to finish
+//      turns the ranges' counts into output offsets.
+//  bp_copy_kernel  each range's hits from scratch to out (a warp per range),
+//      and the total count.  Launched as a programmatic dependent, so its
+//      launch overlaps the stream kernel's tail.
 //
-// X is the larger set (its tile part is split by index and built), Y the
-// smaller (probed; the scratch array is as long as Y).  A consumer whose X
-// elements span 8192 values or more searches each Y element in its X run
-// instead (binary search in shared memory); one with more than 512 Y elements
-// probes them from the ring.
+//  pivot_sample_kernel + pivot_split_kernel  the intersect-path tiles' split
+//      (si_sisi_ip.cu): every S-th element of each set is a pivot; one warp
+//      per pivot finds its rank in the merged pivot order (a merge-path search
+//      over the compact samples) and its exact split in the other set (a
+//      128-element probe at the interpolated position, else a warp search).
+//
+// X is the larger set, Y the smaller (the scratch array is as long as Y).
+// Sets must be sorted and duplicate-free; this engine does not detect
+// unsorted input (si_validate_sorted does).
 #include <algorithm>
 
 #include "si_device.cuh"
@@ -52,7 +43,7 @@
 namespace si {
 namespace {
 
-// ----------------------------------------------------------------- K1 --
+// ------------------------------------------------------------ pivot split --
 // First index i in [lo, hi) with pred(i) true, or hi; pred is monotone
 // (false ... false true ... true).  Warp-cooperative: every lane passes the
 // same lo, hi and gets the same result.  Each round probes 32 evenly spaced
@@ -79,7 +70,7 @@ __device__ __forceinline__ uint64_t warp_first_true(uint64_t lo, uint64_t hi, Pr
     return lo + __popc(fm);
 }
 
-// K1: samples sa[k] = A[k S], sb[k] = B[k S]; clears zero[0, nzero) and the count.
+// Samples sa[k] = A[k S], sb[k] = B[k S]; clears zero[0, nzero) and the count.
 __global__ void __launch_bounds__(256) pivot_sample_kernel(const uint32_t* __restrict__ A, uint64_t nA,
                                                            const uint32_t* __restrict__ B, uint64_t nB, uint64_t S,
                                                            uint32_t* __restrict__ sa, uint32_t* __restrict__ sb,
@@ -135,7 +126,7 @@ __device__ __forceinline__ uint64_t window_rank(const uint32_t* __restrict__ O, 
     return wb + c;
 }
 
-// K2: one warp per pivot rank u in [0, nSA + nSB) (thread 0 also closes the
+// One warp per pivot rank u in [0, nSA + nSB) (thread 0 also closes the
 // table): split_a[u + 1] = #A elements below the pivot's value (exact for an
 // A pivot: its index), split_b[u + 1] likewise.  split[0] = (0, 0) and
 // split[nP + 1] = (nA, nB).  Ties between an A and a B pivot: A first.
@@ -483,11 +474,11 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
     }
 }
 
-// ----------------------------------------------------------------- K5 --
-// Tile t's tile_count[t] hits at scratch[split_y[t] ...] go to
-// out[tile_off[t] ...].  One warp per tile, grid-stride over the tiles; the
-// next tile's count and offsets are loaded while the current one is copied,
-// and each lane keeps 8 loads in flight.  The warp of the last tile writes
+// -------------------------------------------------------------- copy-out --
+// Range t's tile_count[t] hits at scratch[split_y[t] ...] go to
+// out[tile_off[t] ...].  One warp per range, grid-stride over the ranges; the
+// next range's count and offsets are loaded while the current one is copied,
+// and each lane keeps 16 loads in flight.  The warp of the last range writes
 // the total count.
 constexpr int kCopyUnroll = 16;
 __global__ void __launch_bounds__(256) bp_copy_kernel(const uint32_t* __restrict__ tile_count,
@@ -631,7 +622,8 @@ si_status bm_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
     {
         PhaseTimer timer("sisi_split", stream);  // the header (error word) and the count start at zero
         SI_CUDA_TRY(cudaMemsetAsync(w, 0, kHeaderBytes, stream));
-        SI_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), stream));
+        // with element output the copy kernel writes the count; counting adds into it
+        if (!d_out || nX == 0 || nY == 0) SI_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), stream));
     }
     if (nX == 0 || nY == 0) return SI_OK;
     auto launch = [&](auto kernel) -> si_status {

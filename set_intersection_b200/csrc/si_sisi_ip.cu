@@ -519,7 +519,12 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     uint32_t k = 0;            // tiles consumed so far
     for (;; ++k) {
         const uint32_t slot = k % kSlots;
-        if (!mbar_wait_bounded(&full[slot], (k / kSlots) & 1, err, 5, k)) break;
+        bool gave_up = !mbar_wait_bounded(&full[slot], (k / kSlots) & 1, err, 5, k);
+        // Consumers that meet at named barriers (element output, hash probe)
+        // give up together: a warp leaving alone would leave the others at a
+        // barrier it never reaches, which has no time limit.
+        if constexpr (kOut || kInner == kHashProbe) gave_up = named_barrier_or(kConsumerBar, kConsumers, gave_up);
+        if (gave_up) break;
         const InDesc d = in_desc[slot];
         if (d.tile == kEndTile) break;
         const uint32_t* sA = in_ring + d.offA;

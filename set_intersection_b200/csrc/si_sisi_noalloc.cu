@@ -75,3 +75,13 @@ extern "C" si_status si_sisi_noalloc(const uint32_t* dA, uint64_t nA, const uint
     return si::ip_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, scratch, si::kNoAllocScratchBytes,
                        reinterpret_cast<cudaStream_t>(stream));
 }
+
+extern "C" si_status si_sisi_noalloc_check(si_stream_t stream) {
+    // the error words of the library's scratch array, read into host memory:
+    // copies from a symbol allocate nothing
+    uint32_t words[4] = {0, 0, 0, 0};
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    SI_CUDA_TRY(cudaMemcpyFromSymbolAsync(words, si::g_noalloc_scratch, sizeof(words), 0, cudaMemcpyDeviceToHost, s));
+    SI_CUDA_TRY(cudaStreamSynchronize(s));
+    return static_cast<si_status>(words[0]);
+}

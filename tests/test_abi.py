@@ -211,3 +211,26 @@ def test_host_pair_call_checks_arguments_on_host():
     assert L.si_sisi_host(pa, 0, pb, b.size, t, 0, ctypes.byref(cnt), po, out.size, fake,
                           L.si_sisi_host_workspace_size(pa, 0, pb, b.size, t, 0), nul) == Status.OK
     assert cnt.value == 0
+
+
+@pytest.mark.gpu
+def test_bounded_wait_gives_up_and_reports(cuda):
+    """A device wait on a phase that nothing completes gives up after its
+    limit (here 0.2 s), reports SI_ERR_TIMEOUT through the workspace's error
+    word, and the context stays usable for the next call."""
+    import time
+    import torch
+    from set_intersection_b200 import api
+    ws = torch.zeros(64, dtype=torch.int32, device=cuda)
+    nul = ctypes.c_void_p(None)
+    t0 = time.time()
+    assert si.lib.si_wait_selftest(ctypes.c_void_p(ws.data_ptr()), 200_000_000, nul) == Status.TIMEOUT
+    assert time.time() - t0 < 3.0
+    site, detail = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    assert si.lib.si_workspace_diagnostic(ctypes.c_void_p(ws.data_ptr()), nul, ctypes.byref(site),
+                                          ctypes.byref(detail)) == Status.TIMEOUT
+    assert site.value == 31
+    a = torch.arange(0, 1000, 2, dtype=torch.int32, device=cuda)
+    b = torch.arange(0, 1000, 3, dtype=torch.int32, device=cuda)
+    c, _ = api.intersect(a, b, "auto")
+    assert c == 167

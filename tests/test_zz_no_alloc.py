@@ -30,6 +30,14 @@ def test_rejects_pairs_beyond_the_scratch_limit():
     assert lib.si_sisi_noalloc(fake, 10, fake, 10, nul, nul, 0, nul) == Status.INVALID_ARGUMENT
 
 
+def test_documented_limit_fits_the_scratch_array():
+    """The limit |A| + |B| <= 2^29 is what the 4 MiB array holds: the
+    intersect-path workspace of any such pair fits it."""
+    ip = 0  # SI_TECH_IP
+    for na, nb in [(1 << 28, 1 << 28), (1 << 29, 0), (0, 1 << 29), ((1 << 29) - 1, 1)]:
+        assert lib.si_sisi_workspace_size(na, nb, ip) <= 4 << 20, (na, nb)
+
+
 @pytest.mark.gpu
 def test_matches_si_sisi_on_two_calls_in_a_row(cuda):
     import torch
@@ -61,6 +69,11 @@ def test_matches_si_sisi_on_two_calls_in_a_row(cuda):
         assert got_count == want_count
         np.testing.assert_array_equal(out[:got_count].cpu().numpy(), want)
 
+        # ... and with the oracle
+        import oracle
+        np.testing.assert_array_equal(out[:got_count].cpu().numpy().view(np.uint32), oracle.set_intersection(a, b))
+        assert lib.si_sisi_noalloc_check(ctypes.c_void_p(stream.cuda_stream)) == Status.OK
+
         count.fill_(-1)
         st = lib.si_sisi_noalloc(ctypes.c_void_p(da.data_ptr()), a.size, ctypes.c_void_p(db.data_ptr()), b.size,
                                  ctypes.c_void_p(count.data_ptr()), ctypes.c_void_p(None), 0,
@@ -68,3 +81,4 @@ def test_matches_si_sisi_on_two_calls_in_a_row(cuda):
         assert st == Status.OK
         torch.cuda.synchronize(cuda)
         assert int(count.item()) == want_count
+        assert lib.si_sisi_noalloc_check(ctypes.c_void_p(stream.cuda_stream)) == Status.OK
