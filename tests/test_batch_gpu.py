@@ -106,3 +106,28 @@ def test_batched_pool_sample(cuda):
     np.testing.assert_array_equal(count(col, pairs, "auto", table, ws), merge)
     idx = np.random.default_rng(2).choice(len(pairs), 20000, replace=False)
     np.testing.assert_array_equal(merge[idx], oracle.pairs(el, off, off.size - 1, pairs[idx]))
+
+
+@pytest.mark.slow
+def test_batched_config_full_pool(cuda):
+    """The full batched configuration (100000 sets, sizes log-uniform on
+    [32, 2^18] over [0, 2^26), 1M pairs): the tuned batch replayed from its
+    CUDA graph gives every one of the 1M counts the oracle gives."""
+    import os
+    import torch
+    from set_intersection_b200 import api, generate
+    el, off, pairs = generate.batch_pool()
+    col = collection(el, off, (1 << 26) - 1)
+    ws = api.Workspace()
+    dpairs = dev(pairs.astype(np.uint32).view(np.int32))
+    table = api.batch_tune(col, dpairs, workspace=ws)
+    counts = torch.empty(len(pairs), dtype=torch.int32, device=cuda)
+    graph = api.BatchGraph(col, dpairs, counts, "auto", table)
+    try:
+        graph.launch()
+        graph.check()
+        got = counts.cpu().numpy().view(np.uint32)
+    finally:
+        graph.close()
+    want = oracle.pairs(el, off, off.size - 1, pairs, threads=os.cpu_count() or 1)
+    np.testing.assert_array_equal(got, want)
