@@ -97,10 +97,13 @@ def log(*a):
 SKEW_RATIO = 64  # SI_TECH_AUTO: obs when one set is more than this many times the other
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu
-# captures summarised in profiles/: the 2^25 x 2^25 captures (sisi_mid) of the
-# ip tile kernel and of the bitmap engine's bp_stream_kernel, scaled by 8 to
-# the 2^28 x 2^28 launch (ranges, inputs and matches all grow in proportion).
+# captures summarised in profiles/: the bitmap engine's bp_stream_kernel
+# measured at full size (a one-pass dram__bytes capture of the 2^28 x 2^28
+# launch); the ip tile kernel from its 2^25 x 2^25 capture scaled by 8 (tiles,
+# inputs and matches grow in proportion).
 TRAFFIC_PER_LAUNCH = {
+    "bitmap/sisi_large/out": 2.22e9 + 121.57e6,
+    "bitmap/sisi_mid/out": 302.37e6 + 7.99e6,
     "ip/sisi_large/out": 8 * (268.727808e6 + 13.220096e6),
     "ip/sisi_mid/out": 268.727808e6 + 13.220096e6,
 }
