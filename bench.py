@@ -1007,7 +1007,8 @@ def other_workloads(args) -> list:
         out.append({"workload": wl, "metric": d["metric"], "value": d["value"], "unit": d["unit"],
                     "ms_per_step": d["ms_per_step"], "steps": d["steps"],
                     "roofline": {k: roof.get(k) for k in ("bound", "achieved", "peak", "unit", "frac", "kernel",
-                                                           "avg_launch_ms")},
+                                                           "avg_launch_ms", "cublas_int8_tops_measured",
+                                                           "frac_of_cublas_int8") if k in roof},
                     "clocks": d.get("clocks"), **keep, "wall_s": round(time.time() - t0, 1)})
         log(f"{wl} {' '.join(extra)}: {d['value']:.4g} {d['unit']}")
     return out

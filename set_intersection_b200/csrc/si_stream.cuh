@@ -1,0 +1,188 @@
+// si_stream.cuh -- a sorted set read by one warp as a stream of 256-element
+// chunks, and the window bitmaps built from such streams: the building blocks
+// of the single-pair bitmap engine (si_sisi_bitmap.cu) and of the batched
+// pairs' window techniques (si_batch.cu).
+#pragma once
+
+#include <cstdint>
+
+#include "si_device.cuh"
+
+namespace si {
+
+constexpr uint32_t kChunk = 256;                      // elements per chunk: two 16-byte groups per lane
+constexpr uint64_t kMaxStream = (1ull << 32) - 1024;  // stream positions (and 2 chunks ahead) are 32-bit
+
+// One sorted set read by a warp as chunks of 256 elements: lane l holds the
+// 16-byte groups at positions pc + 4 l and pc + 128 + 4 l of a 16-byte aligned
+// base.  Two register buffers alternate (ph = 0: the current chunk is in a,
+// the next one in b), so moving on copies nothing; the chunks four to eight
+// ahead are prefetched into L2 every fourth chunk.  The elements of the stream
+// are positions [v0, v1) (v0 < 4).  Positions before v0 in the first chunk hold
+// a copy of the first element, and positions from v1 on in the last chunk a
+// copy of the last, so every position of a chunk is an element of the set
+// (setting a bit twice is harmless) and nothing checks positions.  Loads past
+// the last group read the last group again (always a valid address).
+// Positions are 32-bit: a stream is shorter than 2^32 - 1024.
+struct SetStream {
+    const uint32_t* base;
+    uint32_t v1, pc, ph;
+    uint4 a0, a1, b0, b1;
+    uint32_t last;  // the current chunk's last element (its largest, in a sorted set)
+};
+
+__device__ __forceinline__ uint4 ld_group(const SetStream& s, uint32_t p) {
+    const uint32_t pend = (s.v1 - 1) & ~3u;  // the last group that holds elements
+    return __ldcs(reinterpret_cast<const uint4*>(s.base + min(p, pend)));
+}
+
+__device__ __forceinline__ uint32_t comp(const uint4& v, uint32_t q) {
+    return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
+}
+
+__device__ __forceinline__ void set_comp(uint4& v, uint32_t q, uint32_t x) {
+    v.x = q == 0 ? x : v.x;
+    v.y = q == 1 ? x : v.y;
+    v.z = q == 2 ? x : v.z;
+    v.w = q == 3 ? x : v.w;
+}
+
+// Lane 0 asks the bulk-copy engine to bring chunks [p, p + 4) (the part that
+// holds elements) into L2; one predicated instruction, no branch.
+__device__ __forceinline__ void prefetch_l2(const SetStream& s, uint32_t p, uint32_t lead) {
+    const uint32_t bytes = (min(p + 4 * kChunk, (s.v1 + 3) & ~3u) - p) * 4;
+    asm volatile("{\n\t.reg .pred l, q;\n\t"
+                 "setp.ne.u32 l, %3, 0;\n\t"
+                 "setp.lt.and.u32 q, %0, %1, l;\n\t"
+                 "@q cp.async.bulk.prefetch.L2.global [%2], %4;\n\t}" ::"r"(p),
+                 "r"(s.v1), "l"(s.base + p), "r"(lead), "r"(bytes)
+                 : "memory");
+}
+
+// The last element of the chunk at pc held in (g0, g1); in the stream's last
+// chunk the positions from v1 on get copies of it.
+__device__ __forceinline__ uint32_t chunk_settle(uint4& g0, uint4& g1, uint32_t pc, uint32_t v1, uint32_t lane) {
+    if (pc + kChunk <= v1) return __shfl_sync(kFullMask, g1.w, 31);
+    const uint32_t lp = v1 - 1 - pc;  // < 256
+    const uint32_t last = __shfl_sync(kFullMask, comp(lp >= 128 ? g1 : g0, lp & 3), (lp & 127) >> 2);
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+        if (pc + 4 * lane + q >= v1) set_comp(g0, q, last);
+        if (pc + 128 + 4 * lane + q >= v1) set_comp(g1, q, last);
+    }
+    return last;
+}
+
+__device__ __forceinline__ void stream_init(SetStream& s, const uint32_t* set, uint64_t i0, uint64_t i1,
+                                            uint32_t lane) {
+    const uint64_t p0 = i0 + ((reinterpret_cast<uintptr_t>(set) & 15u) >> 2);  // from the aligned base below set
+    s.base = set - (p0 - i0) + (p0 & ~uint64_t(3));
+    const uint32_t v0 = static_cast<uint32_t>(p0 & 3);
+    s.v1 = static_cast<uint32_t>(v0 + (i1 - i0));
+    s.pc = 0;
+    s.ph = 0;
+    s.a0 = ld_group(s, 4 * lane);
+    s.a1 = ld_group(s, 128 + 4 * lane);
+    s.b0 = ld_group(s, kChunk + 4 * lane);
+    s.b1 = ld_group(s, kChunk + 128 + 4 * lane);
+    prefetch_l2(s, 2 * kChunk, lane == 0);
+    // the first chunk: positions before v0 get copies of the first element
+    const uint32_t first = __shfl_sync(kFullMask, comp(s.a0, v0), 0);
+    if (lane == 0) {
+#pragma unroll
+        for (uint32_t q = 0; q < 3; ++q)
+            if (q < v0) set_comp(s.a0, q, first);
+    }
+    s.last = chunk_settle(s.a0, s.a1, 0, s.v1, lane);
+}
+
+// Moves to the next chunk (false: there is none); the buffer it leaves takes
+// the chunk after that.  kFromA: the current chunk is in a (ph == 0).
+template <bool kFromA>
+__device__ __forceinline__ bool stream_advance(SetStream& s, uint32_t lane) {
+    if (s.pc + kChunk >= s.v1) return false;
+    s.pc += kChunk;
+    const uint32_t p = s.pc + kChunk + 4 * lane;
+    if constexpr (kFromA) {
+        s.a0 = ld_group(s, p);
+        s.a1 = ld_group(s, p + 128);
+        s.last = chunk_settle(s.b0, s.b1, s.pc, s.v1, lane);
+        s.ph = 1;
+    } else {
+        s.b0 = ld_group(s, p);
+        s.b1 = ld_group(s, p + 128);
+        s.last = chunk_settle(s.a0, s.a1, s.pc, s.v1, lane);
+        s.ph = 0;
+    }
+    if (((s.pc / kChunk) & 3) == 2) prefetch_l2(s, s.pc + 4 * kChunk, lane == 0);
+    return true;
+}
+
+// Sets bit o (< 32 kWords) of the kWords-word bitmap at shared-window address
+// bm, which is aligned to its size: the word's address is one LOP3 of bm and
+// o >> 3.
+template <uint32_t kWords>
+__device__ __forceinline__ void bit_or(uint32_t bm, uint32_t o) {
+    static_assert((kWords & (kWords - 1)) == 0, "the bitmap is a power of two of words");
+    // ordered before the AND pass's loads by the __syncwarp between them
+    asm volatile("red.shared.or.b32 [%0], %1;" ::"r"(bm | ((o >> 3) & (4 * kWords - 4))),
+                 "r"(__funnelshift_l(0u, 1u, o)));
+}
+
+// Sets the bits of the chunk's elements v with a <= v < a + lim (lim = the
+// window, 32 kWords values, or 2^32 - a for the top window, so that no smaller
+// value wraps into it).  bm: shared-window address of the bitmap.
+template <uint32_t kWords>
+__device__ __forceinline__ void chunk_insert(const uint4& g0, const uint4& g1, uint32_t last, uint32_t bm,
+                                             uint32_t a, uint32_t lim) {
+    if (__all_sync(kFullMask, g0.x >= a && last - a < lim)) {  // the whole chunk lies in the window
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) bit_or<kWords>(bm, comp(g0, q) - a);
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) bit_or<kWords>(bm, comp(g1, q) - a);
+    } else {
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) {
+            const uint32_t o0 = comp(g0, q) - a, o1 = comp(g1, q) - a;
+            if (o0 < lim) bit_or<kWords>(bm, o0);
+            if (o1 < lim) bit_or<kWords>(bm, o1);
+        }
+    }
+}
+
+// Inserts the stream's chunks into the bitmap until one reaches past e (it
+// stays current: its later elements belong to later windows); false when the
+// stream ran out.
+template <uint32_t kWords>
+__device__ __forceinline__ bool stream_fill(SetStream& s, uint32_t bm, uint32_t a, uint32_t lim, uint64_t e,
+                                            uint32_t lane) {
+    for (;;) {  // the buffers alternate: a, b, a, ...
+        if (s.ph == 0) {
+            chunk_insert<kWords>(s.a0, s.a1, s.last, bm, a, lim);
+            if (__all_sync(kFullMask, s.last >= e)) return true;
+            if (!stream_advance<true>(s, lane)) return false;
+        }
+        chunk_insert<kWords>(s.b0, s.b1, s.last, bm, a, lim);
+        if (__all_sync(kFullMask, s.last >= e)) return true;
+        if (!stream_advance<false>(s, lane)) return false;
+    }
+}
+
+// The smallest element of the current chunk that is >= e (the chunk's last
+// element is >= e).
+__device__ __forceinline__ uint32_t chunk_first_from(const uint4& g0, const uint4& g1, uint64_t e) {
+    uint32_t m = 0xffffffffu;
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+        const uint32_t v0 = comp(g0, q), v1 = comp(g1, q);
+        m = v0 >= e ? min(m, v0) : m;
+        m = v1 >= e ? min(m, v1) : m;
+    }
+    return __reduce_min_sync(kFullMask, m);
+}
+
+__device__ __forceinline__ uint32_t stream_first_from(const SetStream& s, uint64_t e) {
+    return s.ph == 0 ? chunk_first_from(s.a0, s.a1, e) : chunk_first_from(s.b0, s.b1, e);
+}
+
+}  // namespace si
