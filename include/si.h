@@ -75,11 +75,13 @@ const char* si_last_error_string(void);
  * std::set_intersection orders it.
  *
  * Techniques: IP merges and HI hashes the two sets tile by tile (value-pivot
- * tiles of <= 6144 elements per set, both sets streamed once); BITMAP ANDs
- * the two parts' bitmaps per tile (tiles of <= 16384 elements per set) and
- * orders the output by a scan of the tile counts, through a scratch array as
- * long as the smaller set (so its workspace is about 4 min(nA, nB) bytes
- * larger); OBS searches every element of the smaller set in the larger one
+ * tiles of <= 6144 elements per set for IP, <= 4096 for HI, whose smaller part
+ * always fits its 8192-slot table; both sets streamed once); BITMAP streams
+ * the larger set in equal ranges, one warp per range, with the matching part
+ * of the smaller set, through windows of 16384 values (two bitmaps per warp,
+ * AND and popcount), and orders the output by a scan of the range counts,
+ * through a scratch array as long as the smaller set (so its workspace is
+ * about 4 min(nA, nB) bytes larger); OBS searches every element of the smaller set in the larger one
  * (cached top levels in shared memory); AUTO takes OBS when one set is more
  * than 64 times larger than the other, else BITMAP.
  *
@@ -213,22 +215,40 @@ si_status si_misi(const uint32_t* d_elements, const uint64_t* d_offsets, si_set_
  *
  * d_pairs: device uint32[2 * npairs], pair p = (d_pairs[2p], d_pairs[2p+1]),
  * set indices < k.  d_counts: device uint32[npairs], counts[p] = |S_a ∩ S_b|.
- * t = SI_TECH_IP: every pair by streaming merge; SI_TECH_OBS: every pair by
- * binary search of the smaller set in the larger; SI_TECH_AUTO: per bucket of
- * (log2 smaller size, log2 size ratio) from `table` (host uint8[256],
- * bucket = (min(15, log2 s) << 4) | min(15, log2(l / s)), 0 = merge,
- * 1 = search), or, with table == NULL, search when l >= 16 s.
- * npairs < 2^32.
+ * One technique for every pair: t = SI_TECH_IP (streaming merge), SI_TECH_OBS
+ * (binary search of the smaller set in the larger), SI_TECH_HI (the smaller
+ * set hashed in windows of 1024 elements, the larger probing) or
+ * SI_TECH_BITMAP (AND of two bitmaps per window of 16384 values).
+ * SI_TECH_AUTO: per bucket from `table` (host uint8[SI_BATCH_TABLE_SIZE] of
+ * SI_BATCH_* codes; a code >= SI_BATCH_CODES counts as merge), or, with
+ * table == NULL, search when l >= 16 s and hash otherwise.
+ *   bucket = (d << 8) | (min(15, log2 s) << 4) | min(15, log2(l / s)),
+ * s <= l the two sizes, d the larger set's density class: its mean gap
+ * (last - first) / (l - 1) below 4, 32, 256 or larger (d = 0..3; 3 when
+ * l < 2).  The hash and bitmap techniques run a pair whose larger set has
+ * 2^32 - 1024 elements or more by merge.  npairs < 2^32.
  */
+#define SI_BATCH_TABLE_SIZE 1024
+enum {
+    SI_BATCH_MERGE = 0,       /* streaming merge                              (src/ip.cu) */
+    SI_BATCH_SEARCH = 1,      /* binary search of the smaller set             (src/obs.cu) */
+    SI_BATCH_HASH_1024 = 2,   /* smaller set hashed, windows of 1024 elements (src/hi.cu) */
+    SI_BATCH_HASH_512 = 3,    /* the same, windows of 512 elements */
+    SI_BATCH_BITMAP_16K = 4,  /* window bitmaps of 16384 values               (src/bitmap_dynamic.cu) */
+    SI_BATCH_BITMAP_32K = 5,  /* window bitmaps of 32768 values */
+    SI_BATCH_CODES = 6
+};
 size_t si_batch_workspace_size(uint64_t npairs);
 si_status si_batch_count(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
                          uint64_t npairs, si_technique t, const uint8_t* table, uint32_t* d_counts,
                          void* d_workspace, size_t workspace_bytes, si_stream_t stream);
 
-/* The autotuner: times merge and search on up to `sample` pairs of every
- * bucket that holds at least 32 pairs of this batch and writes the faster
- * choice per bucket to table_out (host uint8[256]; other buckets keep the
- * default).  Synchronises the stream; overwrites d_counts. */
+/* The autotuner: times every SI_BATCH_* technique on up to `sample` pairs of
+ * every bucket that holds at least 32 pairs of this batch and writes the
+ * fastest per bucket to table_out (host uint8[SI_BATCH_TABLE_SIZE]; the
+ * default rule's choice stays unless another is 3 % faster; buckets with
+ * fewer pairs keep the default).  Synchronises the stream; overwrites
+ * d_counts. */
 si_status si_batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
                         uint64_t npairs, uint32_t sample, uint32_t* d_counts, void* d_workspace,
                         size_t workspace_bytes, si_stream_t stream, uint8_t* table_out);
@@ -243,6 +263,20 @@ si_status si_batch_graph_create(const uint32_t* d_elements, const uint64_t* d_of
                                 si_batch_graph** out);
 si_status si_batch_graph_launch(si_batch_graph* graph, si_stream_t stream);
 void si_batch_graph_destroy(si_batch_graph* graph);
+
+/* ------------------------------------------------------ degree statistics --
+ * The per-value and per-set figures of the reference's degree_cdf tool
+ * (src/degree_cdf.cpp:19-62), on the device, for a collection of k sets
+ * holding n_elements elements (d_offsets[k] == n_elements):
+ *   d_inv[v]     = number of sets that hold value v, v < slots (uint32[slots]);
+ *   d_set_sum[s] = sum over the values of set s of d_inv[value] (uint64[k]).
+ * A value >= slots is reported as SI_ERR_INVALID_INPUT in the workspace's
+ * error word.  The sorted lists and running sums of the tool's four files
+ * are formed from these on the host. */
+size_t si_degree_stats_workspace_size(void);
+si_status si_degree_stats(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint64_t n_elements,
+                          uint64_t slots, uint32_t* d_inv, uint64_t* d_set_sum, void* d_workspace,
+                          size_t workspace_bytes, si_stream_t stream);
 
 /* --------------------------------------------------- MISI, dense form --
  * All pairs a < b of a collection of k sets over values 0..universe:

@@ -97,6 +97,8 @@ _SIGNATURES = {
                                      ctypes.POINTER(_vp)]),
     "si_batch_graph_launch": (_int, [_vp, _vp]),
     "si_batch_graph_destroy": (None, [_vp]),
+    "si_degree_stats_workspace_size": (_sz, []),
+    "si_degree_stats": (_int, [_vp, _vp, ctypes.c_uint32, _u64, _u64, _vp, _vp, _vp, _sz, _vp]),
     "si_misi": (_int, [_vp, _vp, SetRange, SetRange, _u64, _int, _vp, _vp, _sz, _vp]),
     "si_misi_dense_workspace_size": (_sz, [ctypes.c_uint32, ctypes.c_uint32, _int]),
     "si_misi_dense": (_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _int, _int, _vp, _vp, _sz, _vp]),

@@ -285,6 +285,35 @@ def misi(col: Collection, tech="bitmap", a_range=None, b_range=None, stride: int
     return counts[:n]
 
 
+# Batched technique codes (the table's bytes) and the table size, as si.h.
+BATCH_TABLE_SIZE = 1024
+BATCH_MERGE, BATCH_SEARCH, BATCH_HASH_1024, BATCH_HASH_512, BATCH_BITMAP_16K, BATCH_BITMAP_32K = range(6)
+BATCH_CODES = 6
+
+
+def _table(table: bytes | None):
+    if table is None:
+        return None
+    if len(table) != BATCH_TABLE_SIZE:
+        raise ValueError(f"a batch table has {BATCH_TABLE_SIZE} bytes")
+    return ctypes.create_string_buffer(bytes(table), BATCH_TABLE_SIZE)
+
+
+def batch_bucket(n_a: int, n_b: int, first_l: int = 0, last_l: int = 0) -> int:
+    """The table index of a pair of sizes n_a, n_b whose larger set runs from
+    first_l to last_l (density class from its mean gap, as the device
+    computes it)."""
+    s, l = min(n_a, n_b), max(n_a, n_b)
+    if l < 2:
+        d = 3
+    else:
+        gap = ((last_l - first_l) & 0xffffffff) // (l - 1)
+        d = 0 if gap < 4 else 1 if gap < 32 else 2 if gap < 256 else 3
+    ls = min(15, s.bit_length() - 1) if s else 0
+    lr = min(15, (l // s).bit_length() - 1) if s else 15
+    return (d << 8) | (ls << 4) | lr
+
+
 def _pairs(pairs: torch.Tensor) -> int:
     if not pairs.is_cuda or pairs.dtype not in (torch.int32, torch.uint32) or not pairs.is_contiguous() or \
             pairs.dim() != 2 or pairs.shape[1] != 2:
@@ -295,14 +324,15 @@ def _pairs(pairs: torch.Tensor) -> int:
 def batch_count_into(col: Collection, pairs: torch.Tensor, counts: torch.Tensor, tech="auto",
                      table: bytes | None = None, workspace: Workspace | None = None, stream=None) -> None:
     """Asynchronous batched call: counts[p] <- |S_a ∩ S_b| for pair p = pairs[p]
-    (tech: "ip" = merge for all, "obs" = search for all, "auto" = per bucket
-    from `table`, the 256-byte output of batch_tune, or the default rule)."""
+    (tech: "ip" = merge, "obs" = search, "hi" = hash, "bitmap" = window
+    bitmaps for every pair; "auto" = per bucket from `table`, the
+    BATCH_TABLE_SIZE-byte output of batch_tune, or the default rule)."""
     n = _pairs(pairs)
     if counts.numel() < n or not counts.is_cuda:
         raise ValueError("counts must be a CUDA tensor of len(pairs) elements")
     ws = workspace if workspace is not None else Workspace(col.elements.device)
     buf = ws.get(lib.si_batch_workspace_size(n))
-    tb = ctypes.create_string_buffer(bytes(table), 256) if table is not None else None
+    tb = _table(table)
     st = lib.si_batch_count(_ptr(col.elements), _ptr(col.offsets), col.k, _ptr(pairs), n, int(technique(tech)),
                             tb, _ptr(counts), _ptr(buf), buf.numel(), _stream(stream))
     check(st, "si_batch_count")
@@ -320,13 +350,14 @@ def batch_count(col: Collection, pairs: torch.Tensor, tech="auto", table: bytes 
 
 def batch_tune(col: Collection, pairs: torch.Tensor, sample: int = 4096, workspace: Workspace | None = None,
                stream=None) -> bytes:
-    """Times merge and search per (size, ratio) bucket of this batch; returns
-    the 256-byte technique table for batch_count(..., "auto", table)."""
+    """Times every batched technique per (density, size, ratio) bucket of
+    this batch; returns the BATCH_TABLE_SIZE-byte technique table for
+    batch_count(..., "auto", table)."""
     n = _pairs(pairs)
     ws = workspace or Workspace(col.elements.device)
     buf = ws.get(lib.si_batch_workspace_size(n))
     counts = torch.empty(max(1, n), dtype=torch.int32, device=col.elements.device)
-    out = ctypes.create_string_buffer(256)
+    out = ctypes.create_string_buffer(BATCH_TABLE_SIZE)
     st = lib.si_batch_tune(_ptr(col.elements), _ptr(col.offsets), col.k, _ptr(pairs), n, sample, _ptr(counts),
                            _ptr(buf), buf.numel(), _stream(stream), out)
     check(st, "si_batch_tune")
@@ -343,7 +374,7 @@ class BatchGraph:
         self.ws = workspace or Workspace(col.elements.device)
         self.buf = self.ws.get(lib.si_batch_workspace_size(n))
         self._keep = (col, pairs, counts)  # the graph holds their addresses
-        tb = ctypes.create_string_buffer(bytes(table), 256) if table is not None else None
+        tb = _table(table)
         h = ctypes.c_void_p()
         st = lib.si_batch_graph_create(_ptr(col.elements), _ptr(col.offsets), col.k, _ptr(pairs), n,
                                        int(technique(tech)), tb, _ptr(counts), _ptr(self.buf), self.buf.numel(),
@@ -367,6 +398,25 @@ class BatchGraph:
             self.close()
         except Exception:
             pass
+
+
+def degree_stats(col: Collection, slots: int, workspace: Workspace | None = None, stream=None,
+                 check_errors: bool = True):
+    """The degree_cdf tool's per-value and per-set figures on the device:
+    (inv, set_sum), inv[v] = number of sets holding v for v < slots (int32
+    holding uint32), set_sum[s] = sum of inv over set s's values (int64)."""
+    ws = workspace or Workspace(col.elements.device)
+    buf = ws.get(lib.si_degree_stats_workspace_size())
+    dev = col.elements.device
+    inv = torch.empty(max(1, slots), dtype=torch.int32, device=dev)
+    set_sum = torch.empty(max(1, col.k), dtype=torch.int64, device=dev)
+    n = col.offsets.numel() and int(col.offsets[-1].item())
+    st = lib.si_degree_stats(_ptr(col.elements), _ptr(col.offsets), col.k, n, slots, _ptr(inv), _ptr(set_sum),
+                             _ptr(buf), buf.numel(), _stream(stream))
+    check(st, "si_degree_stats")
+    if check_errors:
+        ws.check(stream)
+    return inv[:slots], set_sum[:col.k]
 
 
 class HostCollection:

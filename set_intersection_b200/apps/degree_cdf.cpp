@@ -1,6 +1,6 @@
 // degree_cdf: the reference's dataset statistics tool (src/degree_cdf.cpp):
 //
-//   degree_cdf <dataset.bin> <prefix>
+//   degree_cdf <dataset.bin> <prefix> [--device]
 //
 // writes four text files of "first second" lines:
 //   <prefix>_degree_set.txt      (set size, 1-based set id), by set size
@@ -19,7 +19,9 @@
 // itself, the inverted index gets a slot for it (the reference sizes the index
 // `universe` and then writes past its end, src/degree_cdf.cpp:22), so
 // degree_element has a line for that value too.  Counts are 64-bit (the
-// reference's per-set sum is 32-bit).
+// reference's per-set sum is 32-bit).  With --device the inverted-list
+// lengths and the per-set sums come from si_degree_stats on the GPU; the
+// sorts and running sums are the same host code either way.
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
@@ -43,9 +45,39 @@ bool write_pairs(const std::vector<T>& pairs, const std::string& path) {
 
 }  // namespace
 
+// inv[v] and the per-set sums through the library, on the GPU.
+int device_stats(const si_app::Dataset& d, uint64_t slots, std::vector<uint64_t>& inv, std::vector<uint64_t>& sums) {
+    const uint32_t k = d.cardinality;
+    uint32_t *d_el = nullptr, *d_inv = nullptr;
+    uint64_t *d_off = nullptr, *d_sum = nullptr;
+    void* ws = nullptr;
+    const size_t ws_bytes = si_degree_stats_workspace_size();
+    SI_APP_CUDA(cudaMalloc(&d_el, std::max<uint64_t>(d.total, 1) * 4));
+    SI_APP_CUDA(cudaMalloc(&d_off, (uint64_t(k) + 1) * 8));
+    SI_APP_CUDA(cudaMalloc(&d_inv, std::max<uint64_t>(slots, 1) * 4));
+    SI_APP_CUDA(cudaMalloc(&d_sum, std::max<uint64_t>(k, 1) * 8));
+    SI_APP_CUDA(cudaMalloc(&ws, ws_bytes));
+    SI_APP_CUDA(cudaMemcpy(d_el, d.elements.data(), d.total * 4, cudaMemcpyHostToDevice));
+    SI_APP_CUDA(cudaMemcpy(d_off, d.offsets.data(), (uint64_t(k) + 1) * 8, cudaMemcpyHostToDevice));
+    SI_APP_TRY(si_degree_stats(d_el, d_off, k, d.total, slots, d_inv, d_sum, ws, ws_bytes, nullptr));
+    SI_APP_TRY(si_workspace_check(ws, nullptr));
+    std::vector<uint32_t> inv32(slots);
+    sums.assign(k, 0);
+    SI_APP_CUDA(cudaMemcpy(inv32.data(), d_inv, slots * 4, cudaMemcpyDeviceToHost));
+    SI_APP_CUDA(cudaMemcpy(sums.data(), d_sum, uint64_t(k) * 8, cudaMemcpyDeviceToHost));
+    inv.assign(inv32.begin(), inv32.end());
+    cudaFree(d_el);
+    cudaFree(d_off);
+    cudaFree(d_inv);
+    cudaFree(d_sum);
+    cudaFree(ws);
+    return 0;
+}
+
 int main(int argc, char** argv) {
-    if (argc != 3) {
-        std::printf("Usage: %s <dataset.bin> <output prefix>\n", argv[0]);
+    const bool on_device = argc == 4 && std::string(argv[3]) == "--device";
+    if (argc != 3 && !on_device) {
+        std::printf("Usage: %s <dataset.bin> <output prefix> [--device]\n", argv[0]);
         return 1;
     }
     si_app::Dataset d;
@@ -62,18 +94,25 @@ int main(int argc, char** argv) {
     }
     // one slot per value 0 .. universe - 1, and one for `universe` when it occurs
     const uint64_t slots = uint64_t(d.universe) + (d.total && vmax == d.universe ? 1 : 0);
-    // inverted-list lengths: how many sets hold each value
-    std::vector<uint64_t> inv(slots, 0);
-    for (uint64_t e = 0; e < d.total; ++e) ++inv[d.elements[e]];
+    // inverted-list lengths (how many sets hold each value) and, per set,
+    // the sum of its values' lengths
+    std::vector<uint64_t> inv, sums;
+    if (on_device) {
+        if (const int rc = device_stats(d, slots, inv, sums)) return rc;
+    } else {
+        inv.assign(slots, 0);
+        for (uint64_t e = 0; e < d.total; ++e) ++inv[d.elements[e]];
+        sums.assign(d.cardinality, 0);
+        for (uint32_t s = 0; s < d.cardinality; ++s)
+            for (uint64_t e = d.offsets[s]; e < d.offsets[s + 1]; ++e) sums[s] += inv[d.elements[e]];
+    }
     using P32 = std::pair<unsigned int, unsigned int>;
     using P64 = std::pair<unsigned long long, unsigned long long>;
     std::vector<P32> degree_set;
     std::vector<P64> set_cdf;
     for (uint32_t s = 0; s < d.cardinality; ++s) {
-        unsigned long long sum = 0;
-        for (uint64_t e = d.offsets[s]; e < d.offsets[s + 1]; ++e) sum += inv[d.elements[e]];
         degree_set.emplace_back(d.sizes[s], s + 1);
-        set_cdf.emplace_back(d.sizes[s], sum);
+        set_cdf.emplace_back(d.sizes[s], sums[s]);
     }
     std::vector<P32> degree_element;
     std::vector<P64> element_cdf;

@@ -140,8 +140,9 @@ const char* si_last_error_string(void) { return si::g_last_error.c_str(); }
 size_t si_sisi_workspace_size(uint64_t nA, uint64_t nB, si_technique t) {
     switch (t) {
         case SI_TECH_IP:
-        case SI_TECH_HI:
             return si::ip_workspace_size(nA, nB);
+        case SI_TECH_HI:
+            return si::ip_workspace_size(nA, nB, 2);
         case SI_TECH_BITMAP:
             return si::ip_workspace_size(nA, nB, 1);
         case SI_TECH_AUTO:
@@ -213,7 +214,8 @@ size_t si_batch_workspace_size(uint64_t npairs) { return si::batch_workspace_siz
 
 static si_status batch_args(const uint32_t* d_elements, const uint64_t* d_offsets, const uint32_t* d_pairs,
                             uint64_t npairs, si_technique t, uint32_t* d_counts, void* d_workspace) {
-    if (t != SI_TECH_IP && t != SI_TECH_OBS && t != SI_TECH_AUTO) return SI_ERR_INVALID_ARGUMENT;
+    if (t != SI_TECH_IP && t != SI_TECH_OBS && t != SI_TECH_HI && t != SI_TECH_BITMAP && t != SI_TECH_AUTO)
+        return SI_ERR_INVALID_ARGUMENT;
     if (!d_offsets || !d_workspace || (npairs && (!d_pairs || !d_counts))) return SI_ERR_INVALID_ARGUMENT;
     if (npairs >= (1ull << 32)) return SI_ERR_UNSUPPORTED;
     if (!si::aligned(d_elements, 4) || !si::aligned(d_offsets, 8) || !si::aligned(d_pairs, 4) ||
@@ -291,6 +293,21 @@ void si_batch_graph_destroy(si_batch_graph* graph) {
     if (graph->exec) cudaGraphExecDestroy(graph->exec);
     if (graph->graph) cudaGraphDestroy(graph->graph);
     delete graph;
+}
+
+size_t si_degree_stats_workspace_size(void) { return si::degree_workspace_size(); }
+
+si_status si_degree_stats(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint64_t n_elements,
+                          uint64_t slots, uint32_t* d_inv, uint64_t* d_set_sum, void* d_workspace,
+                          size_t workspace_bytes, si_stream_t stream) {
+    if (!d_offsets || !d_workspace || (n_elements && !d_elements) || (slots && !d_inv) || (k && !d_set_sum))
+        return SI_ERR_INVALID_ARGUMENT;
+    if (n_elements && !slots) return SI_ERR_INVALID_ARGUMENT;
+    if (!si::aligned(d_elements, 4) || !si::aligned(d_offsets, 8) || !si::aligned(d_inv, 4) ||
+        !si::aligned(d_set_sum, 8) || !si::aligned(d_workspace, 256))
+        return SI_ERR_INVALID_ARGUMENT;
+    return si::degree_stats(d_elements, d_offsets, k, n_elements, slots, d_inv, d_set_sum, d_workspace,
+                            workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
 }
 
 size_t si_misi_dense_workspace_size(uint32_t k, uint32_t universe, si_technique t) {

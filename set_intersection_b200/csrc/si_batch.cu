@@ -7,11 +7,12 @@
 // counted by ONE persistent kernel:
 //
 //  * Work queue: the pairs are ordered by estimated cost, largest first (a
-//    device radix sort of cost keys), and every warp takes the next pair from
-//    an atomic ticket, so the long pairs start first and the short ones fill
-//    the tail.
-//  * Two techniques per pair, picked per bucket of (log2 of the smaller size,
-//    log2 of the size ratio) from a 256-entry table:
+//    device radix sort of keys that carry each pair's technique), and every
+//    warp takes the next pair from an atomic ticket, so the long pairs start
+//    first and the short ones fill the tail.
+//  * Six technique codes per pair, picked per bucket of (density class of the
+//    larger set, log2 of the smaller size, log2 of the size ratio) from a
+//    1024-entry table:
 //      MERGE (ip): the warp streams both sets through a shared-memory ring of
 //        two 256-element blocks per set; every round finalises the elements up
 //        to the smaller of the two window maxima, counts matches by binary
@@ -20,9 +21,19 @@
 //      SEARCH (obs): the warp takes the smaller set 256 elements at a time,
 //        narrows the window of the larger set that can hold them (two binary
 //        searches), then every lane runs 8 interleaved binary searches in it.
-//  * The table comes from si_batch_tune, which times both techniques on a
-//    sample of every populated bucket, or defaults to SEARCH when the larger
-//    set is at least 16 times the smaller.
+//      HASH (hi, windows of 1024 or 512 elements): the smaller set S is cut
+//        into windows of consecutive elements; each window goes into the
+//        warp's 2048-slot open-addressing table (load <= 1/2 or 1/4) and the
+//        elements of the larger set up to the window's last value probe it
+//        (src/hi.cu:361-418 hashes one partition the same way).
+//      BITMAP (windows of 16384 or 32768 values): both sets set bits in the
+//        warp's two bitmaps of the window's values and the AND's popcount is
+//        the window's count; the next window starts at the larger of the two
+//        sets' next elements (src/bitmap_dynamic.cu:279-319 probes a set's
+//        bitmap; this is the window form of si_sisi_bitmap.cu's engine).
+//    HASH and BITMAP read both sets as 256-element streams (si_stream.cuh).
+//  * The table comes from si_batch_tune, which times every technique on a
+//    sample of every populated bucket, or the default rule.
 #include <algorithm>
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
@@ -30,18 +41,25 @@
 
 #include "si_device.cuh"
 #include "si_internal.h"
+#include "si_stream.cuh"
 
 namespace si {
 namespace {
 
-constexpr int kBThreads = 256;            // 8 warps, 32 KiB of rings
+constexpr int kBThreads = 256;           // 8 warps
 constexpr int kBWarps = kBThreads / 32;
+constexpr int kBCtasPerSm = 3;           // 24 warps per SM (80 registers a thread)
+constexpr uint32_t kWarpSmem = 8192;     // shared bytes per warp: rings, hash table or bitmaps
+constexpr uint32_t kBSmem = kBWarps * kWarpSmem + 4096;  // + the skew to a 4 KiB boundary
 constexpr uint32_t kW = 256;             // window (block) per set per round
 constexpr uint32_t kRing = 2 * kW;       // ring of two blocks per set
 constexpr uint32_t kRingMask = kRing - 1;
 constexpr int kVT = kW / 32;             // elements per lane per block
 constexpr size_t kBatchHeader = 256;     // [0..16) error words, [16] u32 ticket
-constexpr uint8_t kMerge = 0, kSearch = 1;
+// technique codes: the table's bytes (si.h SI_BATCH_*)
+constexpr uint8_t kMerge = 0, kSearch = 1, kHash1024 = 2, kHash512 = 3, kBitmap16K = 4, kBitmap32K = 5;
+constexpr uint8_t kTechCodes = 6;
+constexpr uint32_t kTableSize = 1024;    // 4 density classes x 16 size classes x 16 ratio classes
 
 struct BatchLayout {
     size_t off_keys_in = 0, off_keys = 0, off_cub = 0, cub_bytes = 0, total = 0;
@@ -75,38 +93,71 @@ __host__ __device__ inline uint32_t log2_floor(uint64_t x) {  // x >= 1
 #endif
 }
 
-// Bucket of a pair: (log2 of the smaller size, log2 of larger / smaller), 4 bits each.
-__host__ __device__ inline uint32_t pair_bucket(uint64_t na, uint64_t nb) {
+// Density class of a set from its first and last values and size: the mean
+// gap between consecutive values is < 4, < 32, < 256 or larger (class 0..3).
+__host__ __device__ inline uint32_t density_class(uint32_t first, uint32_t last, uint64_t n) {
+    if (n < 2) return 3;
+    const uint64_t gap = static_cast<uint64_t>(last - first) / (n - 1);
+    return gap < 4 ? 0u : gap < 32 ? 1u : gap < 256 ? 2u : 3u;
+}
+
+// Bucket of a pair: (density class of the larger set, log2 of the smaller
+// size, log2 of larger / smaller): 2 + 4 + 4 bits.
+__host__ __device__ inline uint32_t pair_bucket(uint64_t na, uint64_t nb, uint32_t dclass) {
     const uint64_t s = na < nb ? na : nb, l = na < nb ? nb : na;
     const uint32_t ls = s ? min(15u, log2_floor(s)) : 0u;
     const uint32_t lr = s ? min(15u, log2_floor(l / s)) : 15u;
-    return (ls << 4) | lr;
+    return (dclass << 8) | (ls << 4) | lr;
 }
 
 struct TechTable {
-    uint8_t t[256];
+    uint8_t t[kTableSize];
 };
 
 __device__ __forceinline__ uint64_t search_cost(uint64_t s, uint64_t l) {
     return s * (log2_floor(l + 1) + 4);
 }
 
-// Cost key per pair (descending cost, then pair index): the work queue order.
-__global__ void batch_keys_kernel(const uint64_t* __restrict__ off, const uint32_t* __restrict__ pairs,
-                                  uint64_t npairs, uint32_t k, TechTable table, int forced,
-                                  uint64_t* __restrict__ keys, uint32_t* err) {
+struct PairSets {
+    uint64_t a0, na, b0, nb;
+};
+
+__device__ __forceinline__ PairSets pair_sets(const uint64_t* off, uint32_t a, uint32_t b) {
+    PairSets p;
+    p.a0 = off[a];
+    p.na = off[a + 1] - p.a0;
+    p.b0 = off[b];
+    p.nb = off[b + 1] - p.b0;
+    return p;
+}
+
+// The pair's bucket: its larger set's density class comes from that set's end values.
+__device__ __forceinline__ uint32_t device_bucket(const uint32_t* el, const PairSets& p) {
+    const bool a_large = p.na >= p.nb;
+    const uint64_t l0 = a_large ? p.a0 : p.b0, nl = a_large ? p.na : p.nb;
+    const uint32_t dc = nl >= 2 ? density_class(__ldg(el + l0), __ldg(el + l0 + nl - 1), nl) : 3u;
+    return pair_bucket(p.na, p.nb, dc);
+}
+
+// Queue key per pair: descending cost (28 bits, saturated), technique (4
+// bits), pair index (32 bits); sorted ascending it is the work-queue order.
+__global__ void batch_keys_kernel(const uint32_t* __restrict__ el, const uint64_t* __restrict__ off,
+                                  const uint32_t* __restrict__ pairs, uint64_t npairs, uint32_t k, TechTable table,
+                                  int forced, uint64_t* __restrict__ keys, uint32_t* err) {
     for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < npairs; p += uint64_t(gridDim.x) * blockDim.x) {
         const uint32_t a = pairs[2 * p], b = pairs[2 * p + 1];
         uint64_t cost = 0;
+        uint8_t t = kMerge;
         if (a >= k || b >= k) {
             record_error(err, SI_ERR_INVALID_INPUT, 50, static_cast<uint32_t>(p));
         } else {
-            const uint64_t na = off[a + 1] - off[a], nb = off[b + 1] - off[b];
-            const uint8_t t = forced >= 0 ? static_cast<uint8_t>(forced) : table.t[pair_bucket(na, nb)];
-            cost = t == kSearch ? search_cost(min(na, nb), max(na, nb)) : na + nb;
+            const PairSets ps = pair_sets(off, a, b);
+            t = forced >= 0 ? static_cast<uint8_t>(forced) : table.t[device_bucket(el, ps)];
+            if (t >= kTechCodes) t = kMerge;
+            cost = t == kSearch ? search_cost(min(ps.na, ps.nb), max(ps.na, ps.nb)) : ps.na + ps.nb;
         }
-        const uint64_t c = min(cost, uint64_t(0xffffffffu));
-        keys[p] = (uint64_t(0xffffffffu - c) << 32) | static_cast<uint32_t>(p);
+        const uint64_t c = min(cost, uint64_t(0x0fffffffu));
+        keys[p] = ((uint64_t(0x0fffffffu - c) << 4 | t) << 32) | static_cast<uint32_t>(p);
     }
 }
 
@@ -263,50 +314,245 @@ __device__ uint32_t search_pair(const uint32_t* S, uint64_t ns, const uint32_t* 
     return __reduce_add_sync(kFullMask, hits);
 }
 
+// ---------------------------------------------------------------- HASH --
+constexpr uint32_t kHashSlots = 2048;          // per warp: 8 KiB
+constexpr uint32_t kHashEmpty = 0xffffffffu;   // the empty slot (that value is matched apart)
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t v) {  // Fibonacci hashing to 11 bits
+    return (v * 2654435761u) >> 21;
+}
+
+// Inserts the chunk's elements (8 per lane; repeated values are kept once).
+// A window holds at most kHashSlots / 2 distinct values, so every probe
+// sequence meets an empty slot.
+__device__ __forceinline__ void chunk_hash_insert(uint32_t* tab, const uint4& g0, const uint4& g1) {
+    uint32_t v[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w}, h[8];
+    bool left[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        h[q] = hash_slot(v[q]);
+        const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
+        left[q] = old != kHashEmpty && old != v[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        while (left[q]) {
+            h[q] = (h[q] + 1) & (kHashSlots - 1);
+            const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
+            left[q] = old != kHashEmpty && old != v[q];
+        }
+    }
+}
+
+// Matches of the chunk's elements whose bit is set in `valid` (bit q: g0's
+// component q, bit 4 + q: g1's).  No element is kHashEmpty.
+__device__ __forceinline__ uint32_t chunk_hash_probe(const uint32_t* tab, const uint4& g0, const uint4& g1,
+                                                     uint32_t valid) {
+    const uint32_t v[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+    uint32_t h[8], c = 0;
+    bool left[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        h[q] = hash_slot(v[q]);
+        const uint32_t t = tab[h[q]];
+        const bool on = (valid >> q) & 1u;
+        c += on && t == v[q];
+        left[q] = on && t != v[q] && t != kHashEmpty;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        while (left[q]) {
+            h[q] = (h[q] + 1) & (kHashSlots - 1);
+            const uint32_t t = tab[h[q]];
+            c += t == v[q];
+            left[q] = t != v[q] && t != kHashEmpty;
+        }
+    }
+    return c;
+}
+
+// Which of the chunk at s.pc this lane probes: stream positions in
+// [v0, s.v1) (the head and tail copies are not elements of their own) whose
+// value is <= hi (the later ones belong to the next window).
+__device__ __forceinline__ uint32_t probe_mask(const SetStream& s, const uint4& g0, const uint4& g1, uint32_t v0,
+                                               uint32_t hi, uint32_t lane) {
+    if ((s.pc != 0 || v0 == 0) && s.pc + kChunk <= s.v1 && s.last <= hi) return 0xffu;
+    uint32_t m = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+        const uint32_t p0 = s.pc + 4 * lane + q, p1 = p0 + 128;
+        m |= (p0 >= v0 && p0 < s.v1 && comp(g0, q) <= hi ? 1u : 0u) << q;
+        m |= (p1 >= v0 && p1 < s.v1 && comp(g1, q) <= hi ? 1u : 0u) << (4 + q);
+    }
+    return m;
+}
+
+__device__ __forceinline__ bool stream_next(SetStream& s, uint32_t lane) {
+    return s.ph == 0 ? stream_advance<true>(s, lane) : stream_advance<false>(s, lane);
+}
+
+// HASH: |S ∩ L| (S the smaller set), windows of kWinChunks chunks of S.
+template <uint32_t kWinChunks>
+__device__ uint32_t hash_pair(const uint32_t* S, uint64_t ns, const uint32_t* L, uint64_t nl, uint32_t* tab,
+                              uint32_t lane) {
+    static_assert(kWinChunks * kChunk <= kHashSlots / 2, "a window fills at most half of the table");
+    if (ns == 0 || nl == 0) return 0;
+    // the value 2^32 - 1 marks empty slots: a match of it is counted here and
+    // it leaves both sets (it can only be their last element)
+    const bool s_top = __ldg(S + ns - 1) == kHashEmpty, l_top = __ldg(L + nl - 1) == kHashEmpty;
+    const uint32_t extra = s_top && l_top ? 1u : 0u;
+    ns -= s_top;
+    nl -= l_top;
+    if (ns == 0 || nl == 0) return extra;
+    const uint32_t lo = max(__ldg(S), __ldg(L));
+    if (__ldg(S + ns - 1) < lo || __ldg(L + nl - 1) < lo) return extra;  // value ranges apart
+    const uint64_t s0 = warp_first_true(0, ns, [&](uint64_t i) { return __ldg(S + i) >= lo; });
+    const uint64_t l0 = warp_first_true(0, nl, [&](uint64_t i) { return __ldg(L + i) >= lo; });
+    SetStream ss, sl;
+    stream_init(ss, S, s0, ns, lane);
+    stream_init(sl, L, l0, nl, lane);
+    const uint32_t lv0 = sl.v1 - static_cast<uint32_t>(nl - l0);  // L's first stream position
+    uint4* tab4 = reinterpret_cast<uint4*>(tab);
+    uint32_t hits = 0;
+    for (;;) {
+        for (uint32_t i = lane; i < kHashSlots / 4; i += 32)
+            tab4[i] = make_uint4(kHashEmpty, kHashEmpty, kHashEmpty, kHashEmpty);
+        __syncwarp();
+        // the window: the next kWinChunks chunks of S, up to its last value hi
+        uint32_t hi = 0;
+        bool more_s = true;
+        for (uint32_t c = 0; c < kWinChunks && more_s; ++c) {
+            if (ss.ph == 0)
+                chunk_hash_insert(tab, ss.a0, ss.a1);
+            else
+                chunk_hash_insert(tab, ss.b0, ss.b1);
+            hi = ss.last;
+            more_s = stream_next(ss, lane);
+        }
+        __syncwarp();
+        // L's elements up to hi probe it; a chunk reaching past hi stays
+        bool more_l = true;
+        for (;;) {
+            if (sl.ph == 0)
+                hits += chunk_hash_probe(tab, sl.a0, sl.a1, probe_mask(sl, sl.a0, sl.a1, lv0, hi, lane));
+            else
+                hits += chunk_hash_probe(tab, sl.b0, sl.b1, probe_mask(sl, sl.b0, sl.b1, lv0, hi, lane));
+            if (sl.last > hi) break;
+            more_l = stream_next(sl, lane);
+            if (!more_l) break;
+        }
+        if (!more_l || !more_s) break;
+        __syncwarp();  // the probes are done before the table is cleared
+    }
+    return __reduce_add_sync(kFullMask, hits) + extra;
+}
+
+// -------------------------------------------------------------- BITMAP --
+// BITMAP: |X ∩ Y| by windows of 32 kWords values; bmx: the warp's two
+// kWords-word bitmaps (bmx, bmx + kWords), each aligned to its size.
+template <uint32_t kWords>
+__device__ uint32_t bitmap_pair(const uint32_t* X, uint64_t nx, const uint32_t* Y, uint64_t ny, uint32_t* bmx,
+                                uint32_t lane) {
+    constexpr uint32_t kWinV = 32 * kWords;
+    if (nx == 0 || ny == 0) return 0;
+    const uint32_t lo = max(__ldg(X), __ldg(Y));
+    if (__ldg(X + nx - 1) < lo || __ldg(Y + ny - 1) < lo) return 0;  // value ranges apart
+    uint4* bx4 = reinterpret_cast<uint4*>(bmx);
+    uint4* by4 = reinterpret_cast<uint4*>(bmx + kWords);
+    for (uint32_t i = lane; i < kWords / 2; i += 32) bx4[i] = make_uint4(0u, 0u, 0u, 0u);  // both bitmaps
+    const uint64_t x0 = warp_first_true(0, nx, [&](uint64_t i) { return __ldg(X + i) >= lo; });
+    const uint64_t y0 = warp_first_true(0, ny, [&](uint64_t i) { return __ldg(Y + i) >= lo; });
+    SetStream sx, sy;
+    stream_init(sx, X, x0, nx, lane);
+    stream_init(sy, Y, y0, ny, lane);
+    const uint32_t sbx = smem_addr(bmx), sby = smem_addr(bmx + kWords);
+    uint32_t a = max(__ldg(X + x0), __ldg(Y + y0));
+    uint32_t hits = 0;
+    __syncwarp();
+    for (;;) {
+        const uint64_t e = static_cast<uint64_t>(a) + kWinV;
+        const uint32_t lim = e > 0xffffffffull ? static_cast<uint32_t>(0x100000000ull - a) : kWinV;
+        const bool more_x = stream_fill<kWords>(sx, sbx, a, lim, e, lane);
+        const bool more_y = stream_fill<kWords>(sy, sby, a, lim, e, lane);
+        __syncwarp();
+#pragma unroll
+        for (uint32_t h = 0; h < kWords / 128; ++h) {
+            const uint32_t i = 32 * h + lane;
+            const uint4 p = bx4[i], q = by4[i];
+            bx4[i] = make_uint4(0u, 0u, 0u, 0u);
+            by4[i] = make_uint4(0u, 0u, 0u, 0u);
+            hits += __popc(p.x & q.x) + __popc(p.y & q.y) + __popc(p.z & q.z) + __popc(p.w & q.w);
+        }
+        __syncwarp();
+        if (!more_x || !more_y) break;
+        a = max(stream_first_from(sx, e), stream_first_from(sy, e));
+    }
+    return __reduce_add_sync(kFullMask, hits);
+}
+
+// --------------------------------------------------------------- kernel --
 struct BatchParams {
     const uint32_t* el;
     const uint64_t* off;
     const uint32_t* pairs;
     uint64_t npairs;
     uint32_t k;
-    const uint64_t* keys;  // sorted: low 32 bits = pair index (the queue order)
-    const uint32_t* subset;  // when non-null: the queue is these pair indices, in order
+    const uint64_t* keys;    // sorted queue keys: technique in bits 32..35, pair index in the low 32
+    const uint32_t* subset;  // when non-null: the queue is these pair indices, in order, all by `forced`
     uint32_t* counts;
     uint32_t* ticket;
-    int forced;            // -1: table; else kMerge / kSearch for every pair
-    TechTable table;
+    int forced;
 };
 
-__global__ void __launch_bounds__(kBThreads) batch_kernel(BatchParams p) {
-    __shared__ __align__(16) uint32_t rings[kBWarps][2][kRing];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t* ra = rings[warp][0];
-    uint32_t* rb = rings[warp][1];
+__global__ void __launch_bounds__(kBThreads, kBCtasPerSm) batch_kernel(BatchParams p) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the warp's 8 KiB, 4 KiB aligned (the bitmaps' word addresses are one LOP3)
+    const uint32_t skew = ((smem_addr(smem) + 4095u) & ~4095u) - smem_addr(smem);
+    uint32_t* region = smem + skew / 4 + warp * (kWarpSmem / 4);
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(p.ticket, 1u);
         t = __shfl_sync(kFullMask, t, 0);
         if (t >= p.npairs) break;
-        const uint32_t pi = p.subset ? p.subset[t] : static_cast<uint32_t>(p.keys[t] & 0xffffffffu);
+        uint32_t pi;
+        uint8_t tech;
+        if (p.subset) {
+            pi = p.subset[t];
+            tech = static_cast<uint8_t>(p.forced);
+        } else {
+            const uint64_t key = p.keys[t];
+            pi = static_cast<uint32_t>(key);
+            tech = static_cast<uint8_t>((key >> 32) & 15u);
+        }
         const uint32_t a = p.pairs[2 * uint64_t(pi)], b = p.pairs[2 * uint64_t(pi) + 1];
         if (a >= p.k || b >= p.k) continue;  // recorded by the key kernel
-        const uint64_t a0 = p.off[a], na = p.off[a + 1] - a0, b0 = p.off[b], nb = p.off[b + 1] - b0;
-        const uint8_t tech = p.forced >= 0 ? static_cast<uint8_t>(p.forced) : p.table.t[pair_bucket(na, nb)];
+        const PairSets ps = pair_sets(p.off, a, b);
+        const bool as = ps.na <= ps.nb;  // A is the smaller set
+        const uint32_t* S = p.el + (as ? ps.a0 : ps.b0);
+        const uint32_t* L = p.el + (as ? ps.b0 : ps.a0);
+        const uint64_t ns = as ? ps.na : ps.nb, nl = as ? ps.nb : ps.na;
+        // the stream techniques keep 32-bit positions
+        if (tech >= kHash1024 && nl >= kMaxStream) tech = kMerge;
         uint32_t c;
-        if (tech == kSearch) {
-            const bool as = na <= nb;
-            c = search_pair(p.el + (as ? a0 : b0), as ? na : nb, p.el + (as ? b0 : a0), as ? nb : na, lane);
-        } else {
-            c = merge_pair(p.el + a0, na, p.el + b0, nb, ra, rb, lane);
+        switch (tech) {
+            case kSearch: c = search_pair(S, ns, L, nl, lane); break;
+            case kHash1024: c = hash_pair<4>(S, ns, L, nl, region, lane); break;
+            case kHash512: c = hash_pair<2>(S, ns, L, nl, region, lane); break;
+            case kBitmap16K: c = bitmap_pair<512>(L, nl, S, ns, region, lane); break;
+            case kBitmap32K: c = bitmap_pair<1024>(L, nl, S, ns, region, lane); break;
+            default: c = merge_pair(p.el + ps.a0, ps.na, p.el + ps.b0, ps.nb, region, region + kRing, lane); break;
         }
         if (lane == 0) p.counts[pi] = c;
         __syncwarp();
     }
 }
 
+// Default rule: search when the larger set is at least 16 times the smaller,
+// else hash.
 TechTable default_table() {
     TechTable T;
-    for (uint32_t b = 0; b < 256; ++b) T.t[b] = (b & 15u) >= 4 ? kSearch : kMerge;  // ratio >= 16: search
+    for (uint32_t b = 0; b < kTableSize; ++b) T.t[b] = (b & 15u) >= 4 ? kSearch : kHash1024;
     return T;
 }
 
@@ -332,30 +578,37 @@ si_status batch_launch(const uint32_t* d_elements, const uint64_t* d_offsets, ui
     prm.counts = d_counts;
     prm.ticket = reinterpret_cast<uint32_t*>(w + 16);
     prm.forced = forced;
-    prm.table = table;
     if (!d_subset) {
         PhaseTimer timer("batch_plan", stream);
         const unsigned g = static_cast<unsigned>(std::min<uint64_t>((npairs + 255) / 256, uint64_t(sm_count()) * 8));
-        batch_keys_kernel<<<g, 256, 0, stream>>>(d_offsets, d_pairs, npairs, k, table, forced, keys_in, err);
+        batch_keys_kernel<<<g, 256, 0, stream>>>(d_elements, d_offsets, d_pairs, npairs, k, table, forced, keys_in,
+                                                 err);
         SI_LAUNCH_CHECK("batch_keys_kernel");
         size_t tmp = L.cub_bytes;
         SI_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w + L.off_cub, tmp, keys_in, keys, static_cast<int>(npairs), 0, 64,
                                                    stream));
     }
-    int per_sm = 0;
-    SI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, kBThreads, 0));
-    const unsigned grid = static_cast<unsigned>(sm_count() * std::max(1, per_sm));
+    static int per_sm = [] {
+        int n = 0;
+        if (cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBSmem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel, kBThreads, kBSmem) != cudaSuccess)
+            n = 0;
+        return n;
+    }();
+    if (per_sm == 0) return cuda_fail(cudaGetLastError(), "batch_kernel attributes");
+    const unsigned grid = static_cast<unsigned>(sm_count() * per_sm);
     PhaseTimer timer("batch_count", stream);
-    batch_kernel<<<grid, kBThreads, 0, stream>>>(prm);
+    batch_kernel<<<grid, kBThreads, kBSmem, stream>>>(prm);
     SI_LAUNCH_CHECK("batch_kernel");
     return SI_OK;
 }
 
-__global__ void bucket_kernel(const uint64_t* __restrict__ off, const uint32_t* __restrict__ pairs, uint64_t npairs,
-                              uint32_t k, uint8_t* __restrict__ bucket) {
+__global__ void bucket_kernel(const uint32_t* __restrict__ el, const uint64_t* __restrict__ off,
+                              const uint32_t* __restrict__ pairs, uint64_t npairs, uint32_t k,
+                              uint16_t* __restrict__ bucket) {
     for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < npairs; p += uint64_t(gridDim.x) * blockDim.x) {
         const uint32_t a = pairs[2 * p], b = pairs[2 * p + 1];
-        bucket[p] = (a < k && b < k) ? static_cast<uint8_t>(pair_bucket(off[a + 1] - off[a], off[b + 1] - off[b])) : 0;
+        bucket[p] = (a < k && b < k) ? static_cast<uint16_t>(device_bucket(el, pair_sets(off, a, b))) : 0;
     }
 }
 
@@ -367,8 +620,12 @@ si_status batch_count(const uint32_t* d_elements, const uint64_t* d_offsets, uin
                       uint64_t npairs, si_technique t, const uint8_t* table, uint32_t* d_counts, void* ws,
                       size_t ws_bytes, cudaStream_t stream) {
     TechTable T = default_table();
-    if (table) std::memcpy(T.t, table, 256);
-    const int forced = t == SI_TECH_IP ? kMerge : t == SI_TECH_OBS ? kSearch : -1;
+    if (table) std::memcpy(T.t, table, kTableSize);
+    const int forced = t == SI_TECH_IP       ? kMerge
+                       : t == SI_TECH_OBS    ? kSearch
+                       : t == SI_TECH_HI     ? kHash1024
+                       : t == SI_TECH_BITMAP ? kBitmap16K
+                                             : -1;
     return batch_launch(d_elements, d_offsets, k, d_pairs, npairs, T, forced, nullptr, 0, d_counts, ws, ws_bytes,
                         stream);
 }
@@ -377,37 +634,37 @@ si_status batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint
                      uint64_t npairs, uint32_t sample, uint32_t* d_counts, void* ws, size_t ws_bytes,
                      cudaStream_t stream, uint8_t* table_out) {
     TechTable T = default_table();
-    std::memcpy(table_out, T.t, 256);
+    std::memcpy(table_out, T.t, kTableSize);
     const BatchLayout L = batch_layout(npairs);
     if (ws_bytes < L.total) return SI_ERR_WORKSPACE_TOO_SMALL;
     if (npairs == 0) return SI_OK;
-    // bucket of every pair, on the host
+    // bucket of every pair, on the device, read back
     unsigned char* w = static_cast<unsigned char*>(ws);
-    uint8_t* d_bucket = reinterpret_cast<uint8_t*>(w + L.off_keys_in);  // scratch: npairs bytes
+    uint16_t* d_bucket = reinterpret_cast<uint16_t*>(w + L.off_keys_in);  // scratch: 2 npairs bytes
     const unsigned g = static_cast<unsigned>(std::min<uint64_t>((npairs + 255) / 256, uint64_t(sm_count()) * 8));
-    bucket_kernel<<<g, 256, 0, stream>>>(d_offsets, d_pairs, npairs, k, d_bucket);
+    bucket_kernel<<<g, 256, 0, stream>>>(d_elements, d_offsets, d_pairs, npairs, k, d_bucket);
     SI_LAUNCH_CHECK("bucket_kernel");
-    std::vector<uint8_t> bucket(npairs);
-    SI_CUDA_TRY(cudaMemcpyAsync(bucket.data(), d_bucket, npairs, cudaMemcpyDeviceToHost, stream));
+    std::vector<uint16_t> bucket(npairs);
+    SI_CUDA_TRY(cudaMemcpyAsync(bucket.data(), d_bucket, npairs * 2, cudaMemcpyDeviceToHost, stream));
     SI_CUDA_TRY(cudaStreamSynchronize(stream));
-    std::vector<std::vector<uint32_t>> members(256);
+    std::vector<std::vector<uint32_t>> members(kTableSize);
     for (uint64_t p = 0; p < npairs; ++p)
         if (members[bucket[p]].size() < sample) members[bucket[p]].push_back(static_cast<uint32_t>(p));
-    // sample lists on the device, after the bucket bytes
+    // sample lists on the device, in the queue keys' room
     uint32_t* d_subset = reinterpret_cast<uint32_t*>(w + L.off_keys);  // npairs * 8 bytes of room
     cudaEvent_t e0, e1;
     SI_CUDA_TRY(cudaEventCreate(&e0));
     SI_CUDA_TRY(cudaEventCreate(&e1));
     si_status st = SI_OK;
-    for (int b = 0; b < 256 && st == SI_OK; ++b) {
+    for (uint32_t b = 0; b < kTableSize && st == SI_OK; ++b) {
         const auto& m = members[b];
         if (m.size() < 32) continue;  // too few pairs to matter: keep the default
         if (cudaMemcpyAsync(d_subset, m.data(), m.size() * 4, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
             st = cuda_fail(cudaGetLastError(), "batch_tune copy");
             break;
         }
-        float ms[2] = {0, 0};
-        for (int tech = 0; tech < 2 && st == SI_OK; ++tech) {
+        float ms[kTechCodes] = {};
+        for (uint8_t tech = 0; tech < kTechCodes && st == SI_OK; ++tech) {
             for (int rep = 0; rep < 2 && st == SI_OK; ++rep) {  // the first run warms the caches
                 cudaEventRecord(e0, stream);
                 st = batch_launch(d_elements, d_offsets, k, d_pairs, npairs, T, tech, d_subset, m.size(), d_counts,
@@ -421,7 +678,12 @@ si_status batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint
             }
             cudaEventElapsedTime(&ms[tech], e0, e1);
         }
-        table_out[b] = ms[kSearch] < ms[kMerge] ? kSearch : kMerge;
+        if (st != SI_OK) break;
+        // another technique replaces the default only when it is 3 % faster
+        uint8_t best = T.t[b];
+        for (uint8_t tech = 0; tech < kTechCodes; ++tech)
+            if (ms[tech] < 0.97f * ms[best]) best = tech;
+        table_out[b] = best;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

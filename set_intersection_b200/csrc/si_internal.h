@@ -85,6 +85,10 @@ si_status batch_count(const uint32_t* d_elements, const uint64_t* d_offsets, uin
 si_status batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
                      uint64_t npairs, uint32_t sample, uint32_t* d_counts, void* ws, size_t ws_bytes,
                      cudaStream_t stream, uint8_t* table_out);
+size_t degree_workspace_size();
+si_status degree_stats(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, uint64_t n_elements,
+                       uint64_t slots, uint32_t* d_inv, uint64_t* d_set_sum, void* ws, size_t ws_bytes,
+                       cudaStream_t stream);
 // The dense path's range: MM needs every count exact in f32 (universe < 2^24);
 // BITMAP_NAIVE builds one set's bitmap in shared memory (<= 200 KiB).
 inline bool dense_supported(uint32_t universe, si_technique t) {

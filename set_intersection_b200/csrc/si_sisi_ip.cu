@@ -34,7 +34,11 @@
 namespace si {
 namespace {
 
-constexpr uint32_t kS = 6144;                     // pivot (sample) stride
+// Pivot (sample) stride: a tile holds at most this many elements of each set.
+// The hash probe's tiles are shorter, so that the smaller part of every tile
+// fills at most half of its table.
+__host__ __device__ constexpr uint32_t tile_stride(int inner) { return inner == 2 ? 4096u : 6144u; }
+constexpr uint32_t kS = tile_stride(0);
 constexpr int kPartials = 256;
 
 constexpr uint64_t kFlagAgg = 1ull << 62;
@@ -99,20 +103,25 @@ constexpr int kCtasPerSm = 2;
 constexpr int kSlots = 8;
 constexpr int kOutQ = 16;                    // output descriptors in flight
 constexpr int kGroup = 4;                    // consecutive tiles per scheduling unit (one look-back each)
-constexpr uint32_t kInRing = 14336;          // u32: 56 KiB (the merge path adds the table's area: 72 KiB)
-constexpr uint32_t kOutRing = 8192;          // u32: 32 KiB, a power of two
-constexpr uint32_t kHashSlots = 4096;        // open-addressing table (16 KiB): load factor <= 1/2
-// Shared memory after the rings: the hash table (hash probe).  The merge path
-// needs no table, so its input ring takes that space (about three average
-// tiles instead of two).
+constexpr uint32_t kInRing = 14336;          // u32: 56 KiB (the merge path adds 16 KiB: 72 KiB)
+constexpr uint32_t kHashSlots = 8192;        // open-addressing table (32 KiB): load factor <= 1/2
+// Output ring: a power of two of words holding at least one tile's matches.
+__host__ __device__ constexpr uint32_t out_ring_words(int inner) { return inner == 2 ? 4096u : 8192u; }
+// Shared memory: input ring, output ring, and for the hash probe its table.
+// The merge path needs no table, so its input ring is longer (about three
+// average tiles instead of two); the hash probe's shorter tiles need half the
+// output ring.  Both come to 106.5 KiB: two CTAs per SM.
 __host__ __device__ constexpr uint32_t in_ring_words(int inner) {
-    return inner == 0 ? kInRing + kHashSlots : kInRing;
+    return inner == 0 ? kInRing + 4096u : kInRing;
 }
 __host__ __device__ constexpr size_t smem_bytes(int inner) {
-    return size_t(in_ring_words(inner) + kOutRing + (inner == 2 ? kHashSlots : 0)) * sizeof(uint32_t);
+    return size_t(in_ring_words(inner) + out_ring_words(inner) + (inner == 2 ? kHashSlots : 0)) * sizeof(uint32_t);
 }
-static_assert((kOutRing & (kOutRing - 1)) == 0, "output ring is indexed modulo its size");
-static_assert(kS <= kOutRing, "one tile's matches must fit the output ring");
+static_assert((out_ring_words(0) & (out_ring_words(0) - 1)) == 0 && (out_ring_words(2) & (out_ring_words(2) - 1)) == 0,
+              "output ring is indexed modulo its size");
+static_assert(tile_stride(0) <= out_ring_words(0) && tile_stride(2) <= out_ring_words(2),
+              "one tile's matches must fit the output ring");
+static_assert(tile_stride(2) <= kHashSlots / 2, "a tile's smaller part fills at most half of the hash table");
 constexpr uint32_t kEndTile = 0xffffffffu;
 constexpr uint32_t kConsumerBar = 1;  // named barrier id of the consumer warps
 
@@ -261,16 +270,17 @@ __device__ __forceinline__ ThreadMatches merge_inner(const uint32_t* sA, int na,
 // Hash probe (the reference's hi, src/hi.cu:295-479, restricted to one tile):
 // the smaller set part is inserted into an open-addressing table in shared
 // memory (multiplicative hash, linear probing, load factor <= 1/2), the other
-// part probes it.  A tile whose smaller part exceeds 2048 elements (half the
-// 16 KiB table) takes the merge path, which keeps two CTAs per SM.
+// part probes it.  Tiles hold at most 4096 elements of each set, so every
+// tile's smaller part fits the 8192-slot (32 KiB) table: no tile falls back
+// to the merge path.
 // 0xffffffff marks an empty slot; the value 0xffffffff itself
 // can only be the last element of a part and is carried by a flag instead.
 // The table is cleared at the start of every hash tile, once every consumer
 // thread is past the previous tile's probes (the element-output path's
 // per-tile scan barrier orders that already; count-only needs one more).
 constexpr uint32_t kHashEmpty = 0xffffffffu;
-__device__ __forceinline__ uint32_t hash_slot(uint32_t v) { return (v * 0x9e3779b1u) >> (32 - 12); }
-static_assert(kHashSlots == (1u << 12), "hash_slot yields 12 bits");
+__device__ __forceinline__ uint32_t hash_slot(uint32_t v) { return (v * 0x9e3779b1u) >> (32 - 13); }
+static_assert(kHashSlots == (1u << 13), "hash_slot yields 13 bits");
 
 __device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, const uint32_t* sB, int nb, int tid,
                                                     uint32_t* table, uint32_t* s_has_max, bool need_barrier) {
@@ -322,6 +332,8 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* in_ring = smem;
     constexpr uint32_t kRing = in_ring_words(kInner);
+    constexpr uint32_t kOutRing = out_ring_words(kInner);
+    constexpr uint64_t kTileMax = tile_stride(kInner);
     uint32_t* out_ring = smem + kRing;
     uint32_t* table = smem + kRing + kOutRing;  // hash probe: the hash table
     __shared__ __align__(8) uint64_t full[kSlots], empty[kSlots], ofull[kOutQ], oempty[kOutQ];
@@ -394,7 +406,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
             uint64_t a1 = __shfl_sync(kFullMask, sp_a, lane < kGroup ? lane + 1 : 1);
             uint64_t b0 = __shfl_sync(kFullMask, sp_b, lane < kGroup ? lane : 0);
             uint64_t b1 = __shfl_sync(kFullMask, sp_b, lane < kGroup ? lane + 1 : 1);
-            const bool ok = a0 <= a1 && a1 <= nA && a1 - a0 <= kS && b0 <= b1 && b1 <= nB && b1 - b0 <= kS;
+            const bool ok = a0 <= a1 && a1 <= nA && a1 - a0 <= kTileMax && b0 <= b1 && b1 <= nB && b1 - b0 <= kTileMax;
             const uint64_t t_mine = t_first + lane;
             if (!ok && lane < kGroup && t_mine < nTiles) record_error(err, SI_ERR_INVALID_INPUT);
             if (!ok) a0 = a1 = b0 = b1 = 0;
@@ -530,7 +542,7 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
         const uint32_t* sA = in_ring + d.offA;
         const uint32_t* sB = in_ring + d.offB;
         ThreadMatches tm;
-        if (kInner == kHashProbe && d.na > 0 && d.nb > 0 && min(d.na, d.nb) <= static_cast<int>(kHashSlots / 2)) {
+        if (kInner == kHashProbe && d.na > 0 && d.nb > 0) {
             tm = hash_inner(sA, d.na, sB, d.nb, tid, table, &s_has_max, !kOut);
         } else {
             tm = merge_inner(sA, d.na, sB, d.nb, d.fast != 0, tid);
@@ -612,13 +624,14 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
 }  // namespace
 
 size_t ip_workspace_size(uint64_t nA, uint64_t nB, int inner) {
-    return inner == kBitmapProbe ? bm_workspace_size(nA, nB) : make_layout(nA, nB, kS).total;
+    return inner == kBitmapProbe ? bm_workspace_size(nA, nB) : make_layout(nA, nB, tile_stride(inner)).total;
 }
 
 si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
                   uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream, int inner) {
     if (inner == kBitmapProbe) return bm_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, ws, ws_bytes, stream);
-    const Layout L = make_layout(nA, nB, kS);
+    const uint64_t S = tile_stride(inner);
+    const Layout L = make_layout(nA, nB, S);
     if (ws_bytes < L.total) return SI_ERR_WORKSPACE_TOO_SMALL;
     if (L.nTiles > 0x7fffffffull) return SI_ERR_INVALID_ARGUMENT;
     unsigned char* w = static_cast<unsigned char*>(ws);
@@ -628,8 +641,8 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
     // the split kernel also clears the header, the partial counts and the
     // tiles' look-back status words
     uint32_t* samples_a = reinterpret_cast<uint32_t*>(w + L.off_samples);
-    uint32_t* samples_b = samples_a + align_up(((nA + kS - 1) / kS) * 4, 256) / 4;
-    const si_status sst = pivot_split(dA, nA, dB, nB, kS, split_a, split_b, samples_a, samples_b,
+    uint32_t* samples_b = samples_a + align_up(((nA + S - 1) / S) * 4, 256) / 4;
+    const si_status sst = pivot_split(dA, nA, dB, nB, S, split_a, split_b, samples_a, samples_b,
                                       reinterpret_cast<uint64_t*>(w), L.off_split_a / 8, d_count, stream);
     if (sst != SI_OK) return sst;
 

@@ -13,6 +13,32 @@ namespace si {
 constexpr uint32_t kChunk = 256;                      // elements per chunk: two 16-byte groups per lane
 constexpr uint64_t kMaxStream = (1ull << 32) - 1024;  // stream positions (and 2 chunks ahead) are 32-bit
 
+// First index i in [lo, hi) with pred(i) true, or hi; pred is monotone
+// (false ... false true ... true).  Warp-cooperative: every lane passes the
+// same lo, hi and gets the same result.  Each round probes 32 evenly spaced
+// positions (one per lane) and keeps the gap between the last false and the
+// first true probe.  pred is only evaluated at indices in [lo, hi), and the
+// result stays in [lo, hi] even when pred is not monotone (unsorted input).
+template <class Pred>
+__device__ __forceinline__ uint64_t warp_first_true(uint64_t lo, uint64_t hi, Pred pred) {
+    const uint32_t lane = threadIdx.x & 31;
+    while (hi - lo > 32) {
+        const uint64_t step = (hi - lo + 31) / 32;
+        const uint64_t q = lo + lane * step;
+        const bool valid = q < hi;
+        const uint32_t vm = __ballot_sync(kFullMask, valid);
+        const uint32_t fm = __ballot_sync(kFullMask, valid && !pred(q));
+        const uint32_t c = __popc(fm), nv = __popc(vm);
+        if (c == 0) return lo;
+        const uint64_t new_hi = c < nv ? lo + c * step : hi;
+        lo = lo + (c - 1) * step + 1;
+        hi = new_hi;
+    }
+    const uint64_t q = lo + lane;
+    const uint32_t fm = __ballot_sync(kFullMask, q < hi && !pred(q));
+    return lo + __popc(fm);
+}
+
 // One sorted set read by a warp as chunks of 256 elements: lane l holds the
 // 16-byte groups at positions pc + 4 l and pc + 128 + 4 l of a 16-byte aligned
 // base.  Two register buffers alternate (ph = 0: the current chunk is in a,

@@ -58,6 +58,29 @@ def test_invalid_arguments_rejected_on_host():
     assert L.si_workspace_check(nul, nul) == Status.INVALID_ARGUMENT
 
 
+def test_batch_arguments_and_table_layout_on_host():
+    """si_batch_count takes the four per-pair techniques and AUTO; the table
+    layout (density class, log2 smaller size, log2 ratio) as si.h states it."""
+    from set_intersection_b200 import api
+    L = si.lib
+    nul = ctypes.c_void_p(None)
+    fake = ctypes.c_void_p(0x1000)
+    for t in (Technique.BITMAP_NAIVE, Technique.MM, 42):
+        assert L.si_batch_count(fake, fake, 2, fake, 1, int(t), None, fake, fake, 1 << 20,
+                                nul) == Status.INVALID_ARGUMENT
+    assert L.si_batch_count(fake, fake, 2, fake, 1, int(Technique.IP), None, fake, fake, 64,
+                            nul) != Status.OK
+    assert api.BATCH_TABLE_SIZE == 1024 and api.BATCH_CODES == 6
+    assert api.batch_bucket(100, 100, 0, 99 * 300) == (3 << 8) | (6 << 4) | 0      # gap 300
+    assert api.batch_bucket(100, 1600, 0, 1599 * 3) == (0 << 8) | (6 << 4) | 4     # gap 3, ratio 16
+    assert api.batch_bucket(1600, 100, 10, 10 + 1599 * 31) == (1 << 8) | (6 << 4) | 4
+    assert api.batch_bucket(0, 7, 0, 6000) == (3 << 8) | 15
+    assert api.batch_bucket(5, 1, 0, 4000) == (3 << 8) | (0 << 4) | 2
+    assert api.batch_bucket(1, 1) == (3 << 8) | (0 << 4) | 0
+    with pytest.raises(ValueError):
+        api._table(bytes(256))
+
+
 def test_dense_invalid_arguments_rejected_on_host():
     L = si.lib
     nul = ctypes.c_void_p(None)

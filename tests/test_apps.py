@@ -117,13 +117,9 @@ def test_bin2txt_rejects_truncated_file(apps, tmp_path):
 DEGREE_FILES = ("degree_set", "degree_element", "set_cdf", "element_cdf")
 
 
-@pytest.mark.parametrize("name", ["degree_ties", "degree_zipf"])
-def test_degree_cdf_matches_the_reference_tool(apps, tmp_path, name):
-    """degree_set, degree_element and set_cdf byte-identical to the reference's
-    degree_cdf outputs (tests/golden/<name>_*.txt were made by it); element_cdf
-    holds the element CDF, where the reference writes its set CDF a second time."""
+def _degree_cdf_matches(tmp_path, name, *flags):
     prefix = str(tmp_path / name)
-    r = run("degree_cdf", golden_path(f"{name}.bin"), prefix)
+    r = run("degree_cdf", golden_path(f"{name}.bin"), prefix, *flags)
     assert r.returncode == 0 and "Finished" in r.stdout, r.stdout
     for t in ("degree_set", "degree_element", "set_cdf"):
         assert open(f"{prefix}_{t}.txt").read() == open(golden_path(f"{name}_{t}.txt")).read(), t
@@ -136,8 +132,25 @@ def test_degree_cdf_matches_the_reference_tool(apps, tmp_path, name):
     assert open(f"{prefix}_element_cdf.txt").read() == want
 
 
+@pytest.mark.parametrize("name", ["degree_ties", "degree_zipf"])
+def test_degree_cdf_matches_the_reference_tool(apps, tmp_path, name):
+    """degree_set, degree_element and set_cdf byte-identical to the reference's
+    degree_cdf outputs (tests/golden/<name>_*.txt were made by it); element_cdf
+    holds the element CDF, where the reference writes its set CDF a second time."""
+    _degree_cdf_matches(tmp_path, name)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["degree_ties", "degree_zipf"])
+def test_degree_cdf_on_the_device_matches_the_reference_tool(apps, cuda, tmp_path, name):
+    """The same files with the inverted-list lengths and per-set sums computed
+    by si_degree_stats on the GPU."""
+    _degree_cdf_matches(tmp_path, name, "--device")
+
+
 def test_degree_cdf_usage_and_bad_input(apps, tmp_path):
     assert run("degree_cdf").returncode == 1
+    assert run("degree_cdf", golden_path("degree_ties.bin"), str(tmp_path / "y"), "--gpu").returncode == 1
     bad = tmp_path / "bad.bin"
     bad.write_bytes(open(golden_path("degree_ties.bin"), "rb").read()[:-4])
     assert run("degree_cdf", str(bad), str(tmp_path / "x")).returncode == 1
