@@ -4,20 +4,25 @@
 // The reference has no batched mode: every pair is a host-loop iteration with
 // its own launches (src/ip.cu:141-177 for one tile pair; a single pair costs
 // the 3-kernel SISI path).  Here a list of (a, b) pairs of a CSR collection is
-// counted by ONE persistent kernel:
+// counted by two persistent kernels over one work queue:
 //
 //  * Work queue: the pairs are ordered by estimated cost, largest first (a
-//    device radix sort of keys that carry each pair's technique), and every
-//    warp takes the next pair from an atomic ticket, so the long pairs start
-//    first and the short ones fill the tail.
+//    device radix sort of keys that carry each pair's technique), merge and
+//    search pairs first, hash and bitmap pairs after them; every warp takes
+//    the next pair of its kernel's part from an atomic ticket, so the long
+//    pairs start first and the short ones fill the tail.  The merge / search
+//    kernel runs 32 warps per SM (search is latency-bound), the hash / bitmap
+//    kernel 24 with 8 KiB of shared memory each.
 //  * Six technique codes per pair, picked per bucket of (density class of the
 //    larger set, log2 of the smaller size, log2 of the size ratio) from a
 //    1024-entry table:
 //      MERGE (ip): the warp streams both sets through a shared-memory ring of
 //        two 256-element blocks per set; every round finalises the elements up
-//        to the smaller of the two window maxima, counts matches by binary
-//        search of the A window's elements in the B window, and slides; the
-//        next block of each set is prefetched into registers a round ahead.
+//        to the smaller of the two window maxima and merges them along the
+//        merge path (each lane 16 merged positions after a split search, as
+//        the reference's intersectPath splits a partition, src/ip.cu:207-245),
+//        then slides; the next block of each set is prefetched into registers
+//        a round ahead.
 //      SEARCH (obs): the warp takes the smaller set 256 elements at a time,
 //        narrows the window of the larger set that can hold them (two binary
 //        searches), then every lane runs 8 interleaved binary searches in it.
@@ -48,14 +53,22 @@ namespace {
 
 constexpr int kBThreads = 256;           // 8 warps
 constexpr int kBWarps = kBThreads / 32;
-constexpr int kBCtasPerSm = 3;           // 24 warps per SM (80 registers a thread)
-constexpr uint32_t kWarpSmem = 8192;     // shared bytes per warp: rings, hash table or bitmaps
+// Two kernels share the queue: the merge / search one (64 registers a thread,
+// 32 KiB of rings: 4 CTAs, 32 warps per SM; search is latency-bound and wants
+// the warps) and the stream one for hash and bitmap (80 registers, 8 KiB a
+// warp: 3 CTAs, 24 warps per SM).
+constexpr int kSearchCtasPerSm = 4;
+constexpr int kStreamCtasPerSm = 3;
+constexpr uint32_t kWarpSmem = 8192;     // stream kernel: shared bytes per warp, hash table or bitmaps
 constexpr uint32_t kBSmem = kBWarps * kWarpSmem + 4096;  // + the skew to a 4 KiB boundary
 constexpr uint32_t kW = 256;             // window (block) per set per round
 constexpr uint32_t kRing = 2 * kW;       // ring of two blocks per set
 constexpr uint32_t kRingMask = kRing - 1;
 constexpr int kVT = kW / 32;             // elements per lane per block
-constexpr size_t kBatchHeader = 256;     // [0..16) error words, [16] u32 ticket
+// header: [0..16) error words, [16] u32 ticket of the merge / search kernel,
+// [20] u32 ticket of the stream kernel, [24] u32 pairs in the merge / search
+// part of the queue (its first part)
+constexpr size_t kBatchHeader = 256;
 // technique codes: the table's bytes (si.h SI_BATCH_*)
 constexpr uint8_t kMerge = 0, kSearch = 1, kHash1024 = 2, kHash512 = 3, kBitmap16K = 4, kBitmap32K = 5;
 constexpr uint8_t kTechCodes = 6;
@@ -139,51 +152,44 @@ __device__ __forceinline__ uint32_t device_bucket(const uint32_t* el, const Pair
     return pair_bucket(p.na, p.nb, dc);
 }
 
-// Queue key per pair: descending cost (28 bits, saturated), technique (4
-// bits), pair index (32 bits); sorted ascending it is the work-queue order.
+__host__ __device__ constexpr bool is_stream_tech(uint8_t t) { return t >= kHash1024 && t < kTechCodes; }
+
+// Queue key per pair: stream class (1 bit: hash or bitmap), descending cost
+// (28 bits, saturated), technique (3 bits), pair index (32 bits).  Sorted
+// ascending, the merge / search pairs come first, each part largest first;
+// n_first counts the first part.  A stream technique falls back to merge for
+// a pair whose larger set has 2^32 - 1024 elements or more (stream positions
+// are 32-bit).
 __global__ void batch_keys_kernel(const uint32_t* __restrict__ el, const uint64_t* __restrict__ off,
                                   const uint32_t* __restrict__ pairs, uint64_t npairs, uint32_t k, TechTable table,
-                                  int forced, uint64_t* __restrict__ keys, uint32_t* err) {
-    for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < npairs; p += uint64_t(gridDim.x) * blockDim.x) {
-        const uint32_t a = pairs[2 * p], b = pairs[2 * p + 1];
-        uint64_t cost = 0;
-        uint8_t t = kMerge;
-        if (a >= k || b >= k) {
-            record_error(err, SI_ERR_INVALID_INPUT, 50, static_cast<uint32_t>(p));
-        } else {
-            const PairSets ps = pair_sets(off, a, b);
-            t = forced >= 0 ? static_cast<uint8_t>(forced) : table.t[device_bucket(el, ps)];
-            if (t >= kTechCodes) t = kMerge;
-            cost = t == kSearch ? search_cost(min(ps.na, ps.nb), max(ps.na, ps.nb)) : ps.na + ps.nb;
+                                  int forced, uint64_t* __restrict__ keys, uint32_t* err, uint32_t* n_first) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t end = (npairs + 31) / 32 * 32;  // whole warps, for the aggregated count
+    for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < end; p += stride) {
+        bool first_part = false;
+        if (p < npairs) {
+            const uint32_t a = pairs[2 * p], b = pairs[2 * p + 1];
+            uint64_t cost = 0;
+            uint8_t t = kMerge;
+            if (a >= k || b >= k) {
+                record_error(err, SI_ERR_INVALID_INPUT, 50, static_cast<uint32_t>(p));
+            } else {
+                const PairSets ps = pair_sets(off, a, b);
+                t = forced >= 0 ? static_cast<uint8_t>(forced) : table.t[device_bucket(el, ps)];
+                if (t >= kTechCodes || (is_stream_tech(t) && max(ps.na, ps.nb) >= kMaxStream)) t = kMerge;
+                cost = t == kSearch ? search_cost(min(ps.na, ps.nb), max(ps.na, ps.nb)) : ps.na + ps.nb;
+            }
+            const uint64_t c = min(cost, uint64_t(0x0fffffffu));
+            const uint64_t cls = is_stream_tech(t) ? 1u : 0u;
+            keys[p] = (((cls << 28 | (0x0fffffffu - c)) << 3 | t) << 32) | static_cast<uint32_t>(p);
+            first_part = cls == 0;
         }
-        const uint64_t c = min(cost, uint64_t(0x0fffffffu));
-        keys[p] = ((uint64_t(0x0fffffffu - c) << 4 | t) << 32) | static_cast<uint32_t>(p);
+        const uint32_t m = __ballot_sync(kFullMask, first_part);
+        if ((threadIdx.x & 31) == 0 && m) atomicAdd(n_first, static_cast<uint32_t>(__popc(m)));
     }
 }
 
 // ------------------------------------------------------ per-warp techniques --
-__device__ __forceinline__ uint64_t lower_bound_g(const uint32_t* x, uint64_t lo, uint64_t hi, uint32_t v) {
-    uint64_t len = hi - lo;
-    while (len > 0) {
-        const uint64_t half = len >> 1;
-        const bool c = __ldg(x + lo + half) < v;
-        lo = c ? lo + half + 1 : lo;
-        len = c ? len - half - 1 : half;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ uint64_t upper_bound_g(const uint32_t* x, uint64_t lo, uint64_t hi, uint32_t v) {
-    uint64_t len = hi - lo;
-    while (len > 0) {
-        const uint64_t half = len >> 1;
-        const bool c = __ldg(x + lo + half) <= v;
-        lo = c ? lo + half + 1 : lo;
-        len = c ? len - half - 1 : half;
-    }
-    return lo;
-}
-
 // Block `blk` of x (elements [blk*kW, blk*kW + kW) below n) into registers.
 __device__ __forceinline__ void fetch_block(const uint32_t* x, uint64_t n, uint64_t blk, int lane, uint32_t (&r)[kVT]) {
     const uint64_t b0 = blk * kW;
@@ -241,13 +247,35 @@ __device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B
         // the elements of both windows up to m are final this round
         const uint32_t cA = lastA <= m ? la : ring_upper(ra, ia, la, m);
         const uint32_t cB = lastB <= m ? lb : ring_upper(rb, ib, lb, m);
-#pragma unroll
-        for (int t = 0; t < kVT; ++t) {
-            const uint32_t j = lane + 32u * t;
-            if (j < cA) {
-                const uint32_t v = ra[(ia + j) & kRingMask];
-                const uint32_t q = ring_upper(rb, ib, cB, v);  // elements <= v
-                hits += (q > 0 && rb[(ib + q - 1) & kRingMask] == v) ? 1u : 0u;
+        // merge path over the round's cA + cB (<= 512) final elements: lane l
+        // takes merged positions [16 l, 16 l + 16); ties take the A element
+        // first, and an A element equal to the B element after it is a match
+        {
+            const uint32_t tot = cA + cB;
+            const uint32_t d = min(16u * lane, tot), dend = min(d + 16u, tot);
+            // a = A elements among the first d merged: the first a in
+            // [max(0, d - cB), min(d, cA)] with A[a] > B[d - 1 - a]
+            uint32_t lo = d > cB ? d - cB : 0u, hi = min(d, cA);
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                const bool right = ra[(ia + mid) & kRingMask] <= rb[(ib + d - 1 - mid) & kRingMask];
+                lo = right ? mid + 1 : lo;
+                hi = right ? hi : mid;
+            }
+            uint32_t a = lo, b = d - lo;
+            uint32_t va = a < cA ? ra[(ia + a) & kRingMask] : 0u;
+            uint32_t vb = b < cB ? rb[(ib + b) & kRingMask] : 0u;
+            for (uint32_t x = d; x < dend; ++x) {
+                const bool aok = a < cA, bok = b < cB;
+                const bool takeA = aok && (!bok || va <= vb);
+                hits += (takeA && bok && va == vb) ? 1u : 0u;
+                if (takeA) {
+                    ++a;
+                    va = a < cA ? ra[(ia + a) & kRingMask] : 0u;
+                } else {
+                    ++b;
+                    vb = b < cB ? rb[(ib + b) & kRingMask] : 0u;
+                }
             }
         }
         ia += cA;
@@ -270,20 +298,37 @@ __device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B
     return __reduce_add_sync(kFullMask, hits);
 }
 
-// SEARCH: every element of the smaller set S, binary-searched in the larger L.
-__device__ uint32_t search_pair(const uint32_t* S, uint64_t ns, const uint32_t* L, uint64_t nl, int lane) {
+// SEARCH: every element of the smaller set S, binary-searched in the larger
+// L, 256 elements of S at a time.  The window of L that can hold the block
+// comes from two 32-ary warp searches; a window longer than 512 elements is
+// sampled at 256 evenly spaced positions into shared memory (one load round
+// for the warp, the cached top of the search tree, as the reference's obs
+// caches it, src/obs.cu:275-438), every element finds its gap between two
+// samples there, and only the gap is searched in global memory, 8 searches
+// interleaved per lane.  samp: the warp's 256 words of shared memory.
+constexpr uint32_t kSample = 256;
+__device__ uint32_t search_pair(const uint32_t* S, uint64_t ns, const uint32_t* L, uint64_t nl, uint32_t* samp,
+                               int lane) {
     if (ns == 0 || nl == 0) return 0;
     uint32_t hits = 0;
     uint64_t from = 0;  // the windows advance monotonically
     for (uint64_t base = 0; base < ns; base += kW) {
         const uint64_t last_i = min(base + kW, ns) - 1;
-        // window of L that can hold S[base .. last_i]: lane 0 the lower end, lane 1 the upper
-        uint64_t edge = 0;
-        if (lane == 0) edge = lower_bound_g(L, from, nl, __ldg(S + base));
-        if (lane == 1) edge = upper_bound_g(L, from, nl, __ldg(S + last_i));
-        const uint64_t lo = __shfl_sync(kFullMask, edge, 0), hi = __shfl_sync(kFullMask, edge, 1);
+        const uint32_t v0 = __ldg(S + base), v1 = __ldg(S + last_i);
+        const uint64_t lo = warp_first_true(from, nl, [&](uint64_t i) { return __ldg(L + i) >= v0; });
+        const uint64_t hi = warp_first_true(lo, nl, [&](uint64_t i) { return __ldg(L + i) > v1; });
         from = hi;
         if (lo >= hi) continue;
+        const uint64_t W = hi - lo;
+        const bool sampled = W > 2 * kSample;
+        if (sampled) {
+#pragma unroll
+            for (uint32_t t = 0; t < kSample / 32; ++t) {
+                const uint32_t j = lane + 32 * t;
+                samp[j] = __ldg(L + lo + W * j / kSample);
+            }
+            __syncwarp();
+        }
         uint32_t v[kVT];
         uint64_t pos[kVT], len[kVT];
 #pragma unroll
@@ -291,9 +336,25 @@ __device__ uint32_t search_pair(const uint32_t* S, uint64_t ns, const uint32_t* 
             const uint64_t i = base + lane + 32u * t;
             v[t] = i <= last_i ? __ldg(S + i) : 0u;
             pos[t] = lo;
-            len[t] = i <= last_i ? hi - lo : 0;
+            len[t] = i <= last_i ? W : 0;
         }
-        // interleaved lower-bound searches: kVT independent load chains per lane
+        if (sampled) {
+#pragma unroll
+            for (int t = 0; t < kVT; ++t) {
+                // c = samples <= v; the answer lies between samples c - 1 and c
+                uint32_t c = 0;
+#pragma unroll
+                for (uint32_t step = kSample / 2; step > 0; step >>= 1)
+                    c = samp[c + step - 1] <= v[t] ? c + step : c;
+                c = (c == kSample - 1 && samp[kSample - 1] <= v[t]) ? kSample : c;
+                const uint64_t p0 = lo + W * (c ? c - 1 : 0) / kSample;
+                const uint64_t p1 = c == kSample ? hi : lo + W * c / kSample;
+                pos[t] = p0;
+                len[t] = c == 0 ? 0 : (len[t] ? p1 - p0 : 0);  // c == 0: v is below L[lo]
+            }
+            __syncwarp();  // the samples are read before the next block writes them
+        }
+        // interleaved searches for the last element <= v: kVT independent load chains per lane
         bool more = true;
         while (more) {
             more = false;
@@ -495,35 +556,55 @@ struct BatchParams {
     const uint32_t* el;
     const uint64_t* off;
     const uint32_t* pairs;
-    uint64_t npairs;
     uint32_t k;
-    const uint64_t* keys;    // sorted queue keys: technique in bits 32..35, pair index in the low 32
+    const uint64_t* keys;    // sorted queue keys: technique in bits 32..34, pair index in the low 32
     const uint32_t* subset;  // when non-null: the queue is these pair indices, in order, all by `forced`
+    uint64_t nqueue;         // queue length (all pairs, or the subset)
+    const uint32_t* n_first; // pairs in the queue's first part (merge / search), from the key kernel
     uint32_t* counts;
-    uint32_t* ticket;
+    uint32_t* ticket;        // this kernel's ticket
     int forced;
 };
 
-__global__ void __launch_bounds__(kBThreads, kBCtasPerSm) batch_kernel(BatchParams p) {
+// One kernel per part of the queue.  kStream = false: merge and search pairs
+// (the first part), rings in static shared memory; kStream = true: hash and
+// bitmap pairs (the rest), 8 KiB of dynamic shared memory per warp.  With a
+// subset (the tuner) the kernel of the forced technique takes it all.
+template <bool kStream>
+__global__ void __launch_bounds__(kBThreads, kStream ? kStreamCtasPerSm : kSearchCtasPerSm)
+    batch_kernel(BatchParams p) {
     extern __shared__ __align__(16) uint32_t smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // the warp's 8 KiB, 4 KiB aligned (the bitmaps' word addresses are one LOP3)
-    const uint32_t skew = ((smem_addr(smem) + 4095u) & ~4095u) - smem_addr(smem);
-    uint32_t* region = smem + skew / 4 + warp * (kWarpSmem / 4);
+    // stream kernel: the warp's 8 KiB, 4 KiB aligned (the bitmaps' word
+    // addresses are one LOP3); merge / search kernel: the warp's two rings
+    uint32_t* region;
+    if constexpr (kStream) {
+        const uint32_t skew = ((smem_addr(smem) + 4095u) & ~4095u) - smem_addr(smem);
+        region = smem + skew / 4 + warp * (kWarpSmem / 4);
+    } else {
+        __shared__ __align__(16) uint32_t rings[kBWarps][2 * kRing];
+        region = rings[warp];
+    }
+    uint64_t q0 = 0, q1 = p.nqueue;
+    if (!p.subset) {
+        const uint32_t nf = *p.n_first;
+        q0 = kStream ? nf : 0;
+        q1 = kStream ? p.nqueue : nf;
+    }
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(p.ticket, 1u);
-        t = __shfl_sync(kFullMask, t, 0);
-        if (t >= p.npairs) break;
+        const uint64_t q = q0 + __shfl_sync(kFullMask, t, 0);
+        if (q >= q1) break;
         uint32_t pi;
         uint8_t tech;
         if (p.subset) {
-            pi = p.subset[t];
+            pi = p.subset[q];
             tech = static_cast<uint8_t>(p.forced);
         } else {
-            const uint64_t key = p.keys[t];
+            const uint64_t key = p.keys[q];
             pi = static_cast<uint32_t>(key);
-            tech = static_cast<uint8_t>((key >> 32) & 15u);
+            tech = static_cast<uint8_t>((key >> 32) & 7u);
         }
         const uint32_t a = p.pairs[2 * uint64_t(pi)], b = p.pairs[2 * uint64_t(pi) + 1];
         if (a >= p.k || b >= p.k) continue;  // recorded by the key kernel
@@ -532,16 +613,23 @@ __global__ void __launch_bounds__(kBThreads, kBCtasPerSm) batch_kernel(BatchPara
         const uint32_t* S = p.el + (as ? ps.a0 : ps.b0);
         const uint32_t* L = p.el + (as ? ps.b0 : ps.a0);
         const uint64_t ns = as ? ps.na : ps.nb, nl = as ? ps.nb : ps.na;
-        // the stream techniques keep 32-bit positions
-        if (tech >= kHash1024 && nl >= kMaxStream) tech = kMerge;
         uint32_t c;
-        switch (tech) {
-            case kSearch: c = search_pair(S, ns, L, nl, lane); break;
-            case kHash1024: c = hash_pair<4>(S, ns, L, nl, region, lane); break;
-            case kHash512: c = hash_pair<2>(S, ns, L, nl, region, lane); break;
-            case kBitmap16K: c = bitmap_pair<512>(L, nl, S, ns, region, lane); break;
-            case kBitmap32K: c = bitmap_pair<1024>(L, nl, S, ns, region, lane); break;
-            default: c = merge_pair(p.el + ps.a0, ps.na, p.el + ps.b0, ps.nb, region, region + kRing, lane); break;
+        if constexpr (kStream) {
+            if (nl >= kMaxStream) tech = kMerge;  // only reachable with a tuner subset
+            switch (tech) {
+                case kMerge:
+                    c = merge_pair(p.el + ps.a0, ps.na, p.el + ps.b0, ps.nb, region, region + kRing, lane);
+                    break;
+                case kHash512: c = hash_pair<2>(S, ns, L, nl, region, lane); break;
+                case kBitmap16K: c = bitmap_pair<512>(L, nl, S, ns, region, lane); break;
+                case kBitmap32K: c = bitmap_pair<1024>(L, nl, S, ns, region, lane); break;
+                default: c = hash_pair<4>(S, ns, L, nl, region, lane); break;
+            }
+        } else {
+            if (tech == kSearch)
+                c = search_pair(S, ns, L, nl, region, lane);
+            else
+                c = merge_pair(p.el + ps.a0, ps.na, p.el + ps.b0, ps.nb, region, region + kRing, lane);
         }
         if (lane == 0) p.counts[pi] = c;
         __syncwarp();
@@ -567,39 +655,58 @@ si_status batch_launch(const uint32_t* d_elements, const uint64_t* d_offsets, ui
     if (npairs == 0) return SI_OK;
     uint64_t* keys_in = reinterpret_cast<uint64_t*>(w + L.off_keys_in);
     uint64_t* keys = reinterpret_cast<uint64_t*>(w + L.off_keys);
+    uint32_t* n_first = reinterpret_cast<uint32_t*>(w + 24);
     BatchParams prm;
     prm.el = d_elements;
     prm.off = d_offsets;
     prm.pairs = d_pairs;
-    prm.npairs = d_subset ? nsubset : npairs;
     prm.k = k;
     prm.keys = keys;
     prm.subset = d_subset;
+    prm.nqueue = d_subset ? nsubset : npairs;
+    prm.n_first = n_first;
     prm.counts = d_counts;
-    prm.ticket = reinterpret_cast<uint32_t*>(w + 16);
     prm.forced = forced;
     if (!d_subset) {
         PhaseTimer timer("batch_plan", stream);
         const unsigned g = static_cast<unsigned>(std::min<uint64_t>((npairs + 255) / 256, uint64_t(sm_count()) * 8));
         batch_keys_kernel<<<g, 256, 0, stream>>>(d_elements, d_offsets, d_pairs, npairs, k, table, forced, keys_in,
-                                                 err);
+                                                 err, n_first);
         SI_LAUNCH_CHECK("batch_keys_kernel");
         size_t tmp = L.cub_bytes;
         SI_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w + L.off_cub, tmp, keys_in, keys, static_cast<int>(npairs), 0, 64,
                                                    stream));
     }
-    static int per_sm = [] {
+    static const int search_per_sm = [] {
         int n = 0;
-        if (cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBSmem) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel, kBThreads, kBSmem) != cudaSuccess)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false>, kBThreads, 0) != cudaSuccess) n = 0;
+        return n;
+    }();
+    static const int stream_per_sm = [] {
+        int n = 0;
+        if (cudaFuncSetAttribute(batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBSmem) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<true>, kBThreads, kBSmem) != cudaSuccess)
             n = 0;
         return n;
     }();
-    if (per_sm == 0) return cuda_fail(cudaGetLastError(), "batch_kernel attributes");
-    const unsigned grid = static_cast<unsigned>(sm_count() * per_sm);
+    if (search_per_sm == 0 || stream_per_sm == 0) return cuda_fail(cudaGetLastError(), "batch_kernel attributes");
+    // the subset of the tuner runs in its technique's kernel; the whole queue
+    // in both, one part each (no stream part when every pair merges or searches)
+    const bool forced_stream = forced >= 0 && is_stream_tech(static_cast<uint8_t>(forced));
+    const bool run_search = d_subset ? !forced_stream : true;
+    const bool run_stream = d_subset ? forced_stream : forced < 0 || forced_stream;
     PhaseTimer timer("batch_count", stream);
-    batch_kernel<<<grid, kBThreads, kBSmem, stream>>>(prm);
-    SI_LAUNCH_CHECK("batch_kernel");
+    if (run_search) {
+        prm.ticket = reinterpret_cast<uint32_t*>(w + 16);
+        batch_kernel<false><<<static_cast<unsigned>(sm_count() * search_per_sm), kBThreads, 0, stream>>>(prm);
+        SI_LAUNCH_CHECK("batch_kernel<merge/search>");
+    }
+    if (run_stream) {
+        prm.ticket = reinterpret_cast<uint32_t*>(w + 20);
+        batch_kernel<true><<<static_cast<unsigned>(sm_count() * stream_per_sm), kBThreads, kBSmem, stream>>>(prm);
+        SI_LAUNCH_CHECK("batch_kernel<hash/bitmap>");
+    }
     return SI_OK;
 }
 

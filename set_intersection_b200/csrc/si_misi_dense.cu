@@ -265,21 +265,32 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const uint64_t a = static_cast<uint64_t>(ti) * kTileM + warp * 32 + lane;
     const uint64_t b0 = static_cast<uint64_t>(tj) * kTileN;
     if (done) {
+        // Lane l holds row a = (warp's first row) + l.  Each 32 x 32 block of
+        // counts goes through a padded shared tile (the operand stages are free
+        // once every MMA has completed), so that each store writes 32
+        // consecutive counts of one row.
+        uint32_t* blk = reinterpret_cast<uint32_t*>(stages) + warp * (32 * 33);
+        const uint64_t rowbase = a < k ? tri_index(k, a, a + 1) - (a + 1) : 0;  // index of (a, b) = rowbase + b
+        const uint64_t a_first = static_cast<uint64_t>(ti) * kTileM + warp * 32;
 #pragma unroll 1
-        for (int c = 0; c < kTileN; c += 16) {
-            uint32_t v[16];
-            tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c), v);
-            if (a < k) {
-                const uint64_t rowbase = tri_index(k, a, a + 1) - (a + 1);  // index of (a, b) = rowbase + b
+        for (int c = 0; c < kTileN; c += 32) {
+            uint32_t v[32];
+            tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c),
+                      *reinterpret_cast<uint32_t(*)[16]>(v));
+            tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c + 16),
+                      *reinterpret_cast<uint32_t(*)[16]>(v + 16));
 #pragma unroll
-                for (int x = 0; x < 16; ++x) {
-                    const uint64_t b = b0 + c + x;
-                    if (b > a && b < k) {
-                        const uint32_t cnt = kFp8 ? static_cast<uint32_t>(__uint_as_float(v[x])) : v[x];
-                        counts[rowbase + b] = cnt;
-                    }
-                }
+            for (int x = 0; x < 32; ++x)
+                blk[lane * 33 + x] = kFp8 ? static_cast<uint32_t>(__uint_as_float(v[x])) : v[x];
+            __syncwarp();
+            const uint64_t b = b0 + c + lane;
+#pragma unroll 4
+            for (int r = 0; r < 32; ++r) {
+                const uint64_t ar = a_first + r;
+                const uint64_t base_r = __shfl_sync(kFullMask, rowbase, r);
+                if (ar < k && b > ar && b < k) counts[base_r + b] = blk[r * 33 + lane];
             }
+            __syncwarp();
         }
     }
     tc_fence_before();

@@ -279,21 +279,25 @@ __device__ __forceinline__ ThreadMatches merge_inner(const uint32_t* sA, int na,
 // thread is past the previous tile's probes (the element-output path's
 // per-tile scan barrier orders that already; count-only needs one more).
 constexpr uint32_t kHashEmpty = 0xffffffffu;
+// The whole table is used for every tile: its load stays <= 1/2 and is about
+// 1/4 on average, which keeps probe sequences short (a table sized to each
+// tile's smaller part, load ~1/2, measured 10 % slower on the 2^28 pair).
 __device__ __forceinline__ uint32_t hash_slot(uint32_t v) { return (v * 0x9e3779b1u) >> (32 - 13); }
 static_assert(kHashSlots == (1u << 13), "hash_slot yields 13 bits");
 
 __device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, const uint32_t* sB, int nb, int tid,
                                                     uint32_t* table, uint32_t* s_has_max, bool need_barrier) {
     if (need_barrier) named_barrier(kConsumerBar, kConsumers);
-    uint4* t4 = reinterpret_cast<uint4*>(table);
-    for (uint32_t w = tid; w < kHashSlots / 4; w += kConsumers)
-        t4[w] = make_uint4(kHashEmpty, kHashEmpty, kHashEmpty, kHashEmpty);
-    if (tid == 0) *s_has_max = 0u;
-    named_barrier(kConsumerBar, kConsumers);
     const bool buildA = na <= nb;
     const uint32_t* X = buildA ? sA : sB;
     const uint32_t* Y = buildA ? sB : sA;
     const int nx = buildA ? na : nb, ny = buildA ? nb : na;
+    constexpr uint32_t mask = kHashSlots - 1;
+    uint4* t4 = reinterpret_cast<uint4*>(table);
+    for (uint32_t w = tid; w <= mask / 4; w += kConsumers)
+        t4[w] = make_uint4(kHashEmpty, kHashEmpty, kHashEmpty, kHashEmpty);
+    if (tid == 0) *s_has_max = 0u;
+    named_barrier(kConsumerBar, kConsumers);
     for (int e = tid; e < nx; e += kConsumers) {
         const uint32_t v = X[e];
         if (v == kHashEmpty) {
@@ -301,13 +305,13 @@ __device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, 
             continue;
         }
         uint32_t h = hash_slot(v);
-        while (atomicCAS(table + h, kHashEmpty, v) != kHashEmpty) h = (h + 1) & (kHashSlots - 1);
+        while (atomicCAS(table + h, kHashEmpty, v) != kHashEmpty) h = (h + 1) & mask;
     }
     named_barrier(kConsumerBar, kConsumers);
     const uint32_t has_max = *s_has_max;
     const int r = ((ny + kConsumers - 1) / kConsumers) | 1;
     const int j0 = min(tid * r, ny), j1 = min(j0 + r, ny);
-    uint64_t mask = 0;
+    uint64_t mask64 = 0;
     for (int e = j0; e < j1; ++e) {
         const uint32_t v = Y[e];
         bool hit;
@@ -315,12 +319,12 @@ __device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, 
             hit = has_max != 0;
         } else {
             uint32_t h = hash_slot(v), t;
-            while ((t = table[h]) != v && t != kHashEmpty) h = (h + 1) & (kHashSlots - 1);
+            while ((t = table[h]) != v && t != kHashEmpty) h = (h + 1) & mask;
             hit = t == v;
         }
-        mask |= (hit ? 1ull : 0ull) << (e - j0);
+        mask64 |= (hit ? 1ull : 0ull) << (e - j0);
     }
-    return {Y, j0, mask};
+    return {Y, j0, mask64};
 }
 
 template <bool kOut, int kInner>
