@@ -235,6 +235,7 @@ __device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B
     store_block(rb, 1, lane, pb);
     fetch_block(A, na, 2, lane, pa);
     fetch_block(B, nb, 2, lane, pb);
+
     uint64_t ia = 0, ib = 0, LA = 0, LB = 0;  // LA: first element of the ring's older block
     uint32_t hits = 0;
     __syncwarp();

@@ -56,10 +56,11 @@ constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr size_t kMisiHeader = 256;        // [0..16) error words, [16] u32 ticket
 
 // Partner elements of one work item of a row whose set has `size` elements:
-// staging the set (rebuilt for every item of its row) costs at most a
-// sixteenth of the item's probes (a quarter measured 29 % slower on the
-// power-law collection: the bitmap's inserts are shared atomics).
-constexpr uint64_t kItemPerElement = 16;
+// staging the set (rebuilt for every item of its row) costs at most 1/64 of
+// the item's probes.  Measured on the power-law collection (bitmap probe):
+// 62.8 ms with items of 4x the set, 43.6 with 16x, 39.1 with 32x, 36.8 with
+// 64x: the staging's inserts are shared atomics.
+constexpr uint64_t kItemPerElement = 64;
 __host__ __device__ inline uint64_t item_unit(uint64_t size) {
     return kItemPerElement * size > kMinItemWork ? kItemPerElement * size : kMinItemWork;
 }
