@@ -78,7 +78,7 @@ const char* si_last_error_string(void);
  * tiles of <= 6144 elements per set for IP, <= 4096 for HI, whose smaller part
  * always fits its 8192-slot table; both sets streamed once); BITMAP streams
  * the larger set in equal ranges, one warp per range, with the matching part
- * of the smaller set, through windows of 16384 values (two bitmaps per warp,
+ * of the smaller set, through windows of 32768 values (two bitmaps per warp,
  * AND and popcount), and orders the output by a scan of the range counts,
  * through a scratch array as long as the smaller set (so its workspace is
  * about 4 min(nA, nB) bytes larger); OBS searches every element of the smaller set in the larger one

@@ -206,23 +206,26 @@ __device__ __forceinline__ void store_block(uint32_t* ring, uint64_t blk, int la
     for (int t = 0; t < kVT; ++t) ring[s0 + lane + 32u * t] = r[t];
 }
 
-// Number of window elements w[0 .. len) (ring positions from i0) that are <= v.
-__device__ __forceinline__ uint32_t ring_upper(const uint32_t* ring, uint64_t i0, uint32_t len, uint32_t v) {
+// Number of window elements w[0 .. len) (ring positions from o) that are <= v.
+__device__ __forceinline__ uint32_t ring_upper(const uint32_t* ring, uint32_t o, uint32_t len, uint32_t v) {
     uint32_t lo = 0, n = len;
     while (n > 0) {
         const uint32_t half = n >> 1;
-        const bool c = ring[(i0 + lo + half) & kRingMask] <= v;
+        const bool c = ring[(o + lo + half) & kRingMask] <= v;
         lo = c ? lo + half + 1 : lo;
         n = c ? n - half - 1 : half;
     }
     return lo;
 }
 
-// MERGE: |A ∩ B| by streaming both sets through the warp's rings.
-__device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B, uint64_t nb, uint32_t* ra,
-                               uint32_t* rb, int lane) {
+// MERGE: |A ∩ B| by streaming both sets through the warp's rings: A's at
+// ring[0, kRing), B's at ring[kRing, 2 kRing).  Ring offsets are 32-bit.
+__device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B, uint64_t nb, uint32_t* ring,
+                               int lane) {
     if (na == 0 || nb == 0) return 0;
     if (__ldg(A + na - 1) < __ldg(B) || __ldg(B + nb - 1) < __ldg(A)) return 0;  // disjoint value ranges
+    uint32_t* ra = ring;
+    uint32_t* rb = ring + kRing;
     uint32_t pa[kVT], pb[kVT];
     // blocks 0 and 1 of each set into the rings, block 2 into registers
     fetch_block(A, na, 0, lane, pa);
@@ -243,11 +246,12 @@ __device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B
         const uint32_t la = na - ia < kW ? static_cast<uint32_t>(na - ia) : kW;
         const uint32_t lb = nb - ib < kW ? static_cast<uint32_t>(nb - ib) : kW;
         if (la == 0 || lb == 0) break;
-        const uint32_t lastA = ra[(ia + la - 1) & kRingMask], lastB = rb[(ib + lb - 1) & kRingMask];
+        const uint32_t oa = static_cast<uint32_t>(ia) & kRingMask, ob = static_cast<uint32_t>(ib) & kRingMask;
+        const uint32_t lastA = ra[(oa + la - 1) & kRingMask], lastB = rb[(ob + lb - 1) & kRingMask];
         const uint32_t m = min(lastA, lastB);
         // the elements of both windows up to m are final this round
-        const uint32_t cA = lastA <= m ? la : ring_upper(ra, ia, la, m);
-        const uint32_t cB = lastB <= m ? lb : ring_upper(rb, ib, lb, m);
+        const uint32_t cA = lastA <= m ? la : ring_upper(ra, oa, la, m);
+        const uint32_t cB = lastB <= m ? lb : ring_upper(rb, ob, lb, m);
         // merge path over the round's cA + cB (<= 512) final elements: lane l
         // takes merged positions [16 l, 16 l + 16); ties take the A element
         // first, and an A element equal to the B element after it is a match
@@ -259,23 +263,24 @@ __device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B
             uint32_t lo = d > cB ? d - cB : 0u, hi = min(d, cA);
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
-                const bool right = ra[(ia + mid) & kRingMask] <= rb[(ib + d - 1 - mid) & kRingMask];
+                const bool right = ra[(oa + mid) & kRingMask] <= rb[(ob + d - 1 - mid) & kRingMask];
                 lo = right ? mid + 1 : lo;
                 hi = right ? hi : mid;
             }
             uint32_t a = lo, b = d - lo;
-            uint32_t va = a < cA ? ra[(ia + a) & kRingMask] : 0u;
-            uint32_t vb = b < cB ? rb[(ib + b) & kRingMask] : 0u;
-            for (uint32_t x = d; x < dend; ++x) {
-                const bool aok = a < cA, bok = b < cB;
-                const bool takeA = aok && (!bok || va <= vb);
-                hits += (takeA && bok && va == vb) ? 1u : 0u;
-                if (takeA) {
-                    ++a;
-                    va = a < cA ? ra[(ia + a) & kRingMask] : 0u;
-                } else {
-                    ++b;
-                    vb = b < cB ? rb[(ib + b) & kRingMask] : 0u;
+            uint32_t va = ra[(oa + a) & kRingMask], vb = rb[(ob + b) & kRingMask];
+            // branch-free steps; a value read past cA or cB is never used
+#pragma unroll
+            for (uint32_t x = 0; x < 16; ++x) {
+                if (d + x < dend) {
+                    const bool aok = a < cA, bok = b < cB;
+                    const bool takeA = aok && (!bok || va <= vb);
+                    hits += (takeA && bok && va == vb) ? 1u : 0u;
+                    a += takeA ? 1u : 0u;
+                    b += takeA ? 0u : 1u;
+                    const uint32_t v = ring[takeA ? ((oa + a) & kRingMask) : (kRing + ((ob + b) & kRingMask))];
+                    va = takeA ? v : va;
+                    vb = takeA ? vb : v;
                 }
             }
         }
@@ -619,7 +624,7 @@ __global__ void __launch_bounds__(kBThreads, kStream ? kStreamCtasPerSm : kSearc
             if (nl >= kMaxStream) tech = kMerge;  // only reachable with a tuner subset
             switch (tech) {
                 case kMerge:
-                    c = merge_pair(p.el + ps.a0, ps.na, p.el + ps.b0, ps.nb, region, region + kRing, lane);
+                    c = merge_pair(p.el + ps.a0, ps.na, p.el + ps.b0, ps.nb, region, lane);
                     break;
                 case kHash512: c = hash_pair<2>(S, ns, L, nl, region, lane); break;
                 case kBitmap16K: c = bitmap_pair<512>(L, nl, S, ns, region, lane); break;
@@ -630,7 +635,7 @@ __global__ void __launch_bounds__(kBThreads, kStream ? kStreamCtasPerSm : kSearc
             if (tech == kSearch)
                 c = search_pair(S, ns, L, nl, region, lane);
             else
-                c = merge_pair(p.el + ps.a0, ps.na, p.el + ps.b0, ps.nb, region, region + kRing, lane);
+                c = merge_pair(p.el + ps.a0, ps.na, p.el + ps.b0, ps.nb, region, lane);
         }
         if (lane == 0) p.counts[pi] = c;
         __syncwarp();

@@ -38,6 +38,7 @@
 
 #include "si_device.cuh"
 #include "si_internal.h"
+#include "si_stream.cuh"
 
 namespace si {
 namespace {
@@ -52,6 +53,7 @@ constexpr uint32_t kHashBits = 14;
 static_assert(kHashTable == (1u << kHashBits), "hash table size");
 constexpr uint64_t kMinItemWork = 131072;  // partner elements per work item, at least
 constexpr uint32_t kLaneCol = 64;          // partner pieces below this size are probed by one lane each
+constexpr uint64_t kMinSlice = 4096;       // partner elements per slice a warp takes, at least
 constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr size_t kMisiHeader = 256;        // [0..16) error words, [16] u32 ticket
 
@@ -262,6 +264,7 @@ template <int kTech>
 __global__ void __launch_bounds__(kMisiThreads, misi_ctas_per_sm(kTech)) misi_probe_kernel(MisiParams p) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint64_t s_item;
+    __shared__ unsigned long long s_next;  // the next slice of the item's partner elements
     __shared__ uint32_t s_has_max;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t rows = p.nA + p.nB;
@@ -291,15 +294,14 @@ __global__ void __launch_bounds__(kMisiThreads, misi_ctas_per_sm(kTech)) misi_pr
         const uint64_t x0 = p.off[x_id], nx = p.off[x_id + 1] - x0;
         const uint32_t* x = p.el + x0;
         // partner elements are numbered by Pt (prefix sums of the sorted
-        // sizes); this item takes [it_lo, it_hi), warp w an equal share of it
+        // sizes); this item takes [it_lo, it_hi), and the warps take slices
+        // of it from a shared counter (at least 4 per warp), so that a warp
+        // whose slices probe faster takes more of them
         const uint64_t unit = item_unit(nx);
         const uint64_t it_lo = Pt[c_row] + seg * unit;
         const uint64_t it_hi = min(it_lo + unit, Pt[nt]);
         const uint64_t span_e = it_hi - it_lo;
-        const uint64_t w_lo = it_lo + span_e * warp / kMisiWarps;
-        const uint64_t w_hi = it_lo + span_e * (warp + 1) / kMisiWarps;
-        // the partner holding element w_lo: last c with Pt[c] <= w_lo
-        const uint32_t c_first = static_cast<uint32_t>(lower_bound_u64(Pt, c_row, nt + 1, w_lo + 1) - 1);
+        const uint64_t slice = max(kMinSlice, span_e / (4 * kMisiWarps));
 
         // ---- chunks of x ----
         uint64_t i0 = 0;
@@ -342,11 +344,21 @@ __global__ void __launch_bounds__(kMisiThreads, misi_ctas_per_sm(kTech)) misi_pr
             const uint32_t m = static_cast<uint32_t>(i1 - i0);
             const uint32_t vlast = __ldg(x + i1 - 1);
             const bool single = i0 == 0 && i1 == nx;
+            if (tid == 0) s_next = it_lo;
             __syncthreads();
             const bool has_max = kTech == SI_TECH_HI ? s_has_max != 0 : false;
 
-            // ---- this warp's slice [w_lo, w_hi), 32 partners at a time:
-            // lane q takes partner c + q's piece of the slice ----
+            for (;;) {
+            // ---- a slice [w_lo, w_hi), 32 partners at a time: lane q takes
+            // partner c + q's piece of the slice ----
+            unsigned long long w_lo = 0;
+            if (lane == 0) w_lo = atomicAdd(&s_next, static_cast<unsigned long long>(slice));
+            w_lo = __shfl_sync(kFullMask, w_lo, 0);
+            if (w_lo >= it_hi) break;
+            const uint64_t w_hi = min(static_cast<uint64_t>(w_lo) + slice, it_hi);
+            // the partner holding element w_lo: last c with Pt[c] <= w_lo
+            const uint32_t c_first =
+                static_cast<uint32_t>(warp_first_true(c_row, nt + 1, [&](uint64_t q) { return Pt[q] > w_lo; }) - 1);
             uint64_t e = w_lo;
             uint32_t c = c_first;
             while (e < w_hi) {
@@ -467,6 +479,7 @@ __global__ void __launch_bounds__(kMisiThreads, misi_ctas_per_sm(kTech)) misi_pr
                 }
                 e = __shfl_sync(kFullMask, pe, nb - 1);
                 c += nb;
+            }
             }
             __syncthreads();  // the structure is rebuilt for the next chunk / item
             i0 = i1;
