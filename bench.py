@@ -102,8 +102,8 @@ SKEW_RATIO = 64  # SI_TECH_AUTO: obs when one set is more than this many times t
 # launch); the ip tile kernel from its 2^25 x 2^25 capture scaled by 8 (tiles,
 # inputs and matches grow in proportion).
 TRAFFIC_PER_LAUNCH = {
-    "bitmap/sisi_large/out": 2.22e9 + 121.57e6,
-    "bitmap/sisi_mid/out": 302.37e6 + 7.99e6,
+    "bitmap/sisi_large/out": 2.246e9 + 121.53e6,   # one-pass dram__bytes capture of the 2^28 stream kernel
+    "bitmap/sisi_mid/out": 321.59e6 + 5.21e6,      # from the 2^25 full capture
     "ip/sisi_large/out": 8 * (268.727808e6 + 13.220096e6),
     "ip/sisi_mid/out": 268.727808e6 + 13.220096e6,
 }
@@ -855,7 +855,7 @@ def run_ours_batch(args, rank: int, world: int):
     dpairs = torch.from_numpy(pairs.view(np.int32)).to(dev)
     counts = torch.empty(npairs, dtype=torch.int32, device=dev)
     ws = api.Workspace(dev)
-    tech = args.technique if args.technique in ("ip", "obs", "auto") else "auto"
+    tech = args.technique if args.technique in ("ip", "obs", "hi", "bitmap", "auto") else "auto"
 
     t0 = time.perf_counter()
     table = api.batch_tune(col, dpairs, workspace=ws, stream=stream) if tech == "auto" else None
@@ -902,6 +902,31 @@ def run_ours_batch(args, rank: int, world: int):
     lib.si_timer_read(b"batch_count", ctypes.byref(k_ms), ctypes.byref(k_n))
     lib.si_timer_reset()
     kern_ms = k_ms.value / max(1, k_n.value)
+
+    # every populated bucket alone, each technique code (a table holding that
+    # code for every bucket): what the tuner measures, on all of a bucket's pairs
+    bucket_times = None
+    if args.bucket_times and rank == 0:
+        bk = api.batch_buckets(el, off, pairs)
+        cbuf = torch.empty(npairs, dtype=torch.int32, device=dev)
+        bucket_times = []
+        for b in np.unique(bk):
+            idx = np.nonzero(bk == b)[0]
+            if len(idx) < 200:
+                continue
+            sub = dpairs[torch.from_numpy(idx).to(dev)].contiguous()
+            row = {"bucket": int(b), "density": int(b >> 8), "log2_small": int((b >> 4) & 15),
+                   "log2_ratio": int(b & 15), "pairs": int(len(idx)), "ms": []}
+            for code in range(api.BATCH_CODES):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                for _ in range(2):  # the second run is timed
+                    e0.record(stream)
+                    api.batch_count_into(col, sub, cbuf, "auto", bytes([code]) * api.BATCH_TABLE_SIZE, ws, stream)
+                    e1.record(stream)
+                e1.synchronize()
+                row["ms"].append(round(e0.elapsed_time(e1), 4))
+            bucket_times.append(row)
+            log(f"bucket {row['log2_small']},{row['log2_ratio']} d{row['density']} n={row['pairs']}: {row['ms']}")
 
     # plain: one single-pair call per pair (3 launches each), on a sample
     plain = None
@@ -972,7 +997,12 @@ def run_ours_batch(args, rank: int, world: int):
     if world == 1 and not args.no_cpu_baseline:
         kind, threads, cval, desc, _ = batch_cpu_measure(el, off, pairs, 20000, steps=3, warmup=1)
         cpu = {"value": cval, "unit": "pairs/s", "cores": threads, "kind": kind, "sample": desc}
-    tb = np.frombuffer(table, np.uint8) if table is not None else None
+    codes_used = None
+    if table is not None:
+        tb = np.frombuffer(table, np.uint8)
+        per_pair = tb[api.batch_buckets(el, off, pairs)]
+        names = ["merge", "search", "hash_1024", "hash_512", "bitmap_16k", "bitmap_32k"]
+        codes_used = {names[c]: int((per_pair == c).sum()) for c in range(api.BATCH_CODES) if (per_pair == c).any()}
     line = {
         "metric": "batched pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -980,18 +1010,23 @@ def run_ours_batch(args, rank: int, world: int):
         "config": {"workload": args.workload, "desc": w["desc"], "technique": tech, "k": k, "pairs": npairs,
                    "elements": int(el.size), "merge_elements": merge_elems,
                    "l2": f"pool {el.size * 4 >> 20} MiB > 126 MB L2; no flush",
-                   "graph": "one CUDA graph per step: key kernel, radix sort of the queue, batch kernel",
+                   "graph": "one CUDA graph per step: key kernel, radix sort of the queue, the merge/search and "
+                            "hash/bitmap batch kernels",
                    "autotune_s": tune_s if table is not None else None,
-                   "search_buckets": int(tb.sum()) if tb is not None else None,
+                   "pairs_per_technique": codes_used,
                    "parallelism": f"replicas{world}", "parity_vs_oracle": parity,
                    "plain_per_pair": plain,
                    "speedup_vs_plain": (value / world / plain["pairs_per_s"]) if plain else None},
         "roofline": roof,
         "e2e": e2e,
-        "gpu_launches": 2 * args.steps,
+        # ours per step: the key kernel and one or two batch kernels (the sort is CUB's)
+        "gpu_launches": (2 if tech in ("ip", "obs") else 3) * args.steps,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
     }
+    if bucket_times is not None:
+        line["bucket_times"] = {"codes": ["merge", "search", "hash_1024", "hash_512", "bitmap_16k", "bitmap_32k"],
+                                "buckets": bucket_times}
     print(json.dumps(line), flush=True)
     rep.close()
 
@@ -1046,6 +1081,8 @@ def main():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-parity", action="store_true")
+    p.add_argument("--bucket-times", action="store_true",
+                   help="batch: also time every technique code on every bucket of 200 pairs or more")
     p.add_argument("--no-plain", action="store_true",
                    help="dense / batch: skip timing the plain kernel (popcount / one call per pair)")
     p.add_argument("--dtype", choices=["int8", "fp8"], default="int8", help="dense: tensor-core operand type")

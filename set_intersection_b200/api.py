@@ -314,6 +314,30 @@ def batch_bucket(n_a: int, n_b: int, first_l: int = 0, last_l: int = 0) -> int:
     return (d << 8) | (ls << 4) | lr
 
 
+def batch_buckets(elements, offsets, pairs):
+    """batch_bucket of every pair of a host CSR collection (numpy arrays:
+    uint32 elements, int64 offsets, uint32 pairs [n, 2]): int array [n]."""
+    import numpy as np
+    off = np.asarray(offsets, dtype=np.int64)
+    el = np.asarray(elements, dtype=np.uint32)
+    sz = np.diff(off)
+    p = np.asarray(pairs, dtype=np.int64)
+    na, nb = sz[p[:, 0]], sz[p[:, 1]]
+    s, l = np.minimum(na, nb), np.maximum(na, nb)
+    larger = np.where(na >= nb, p[:, 0], p[:, 1])
+    if el.size:
+        first = el[np.minimum(off[larger], el.size - 1)].astype(np.int64)
+        last = el[np.clip(off[larger + 1] - 1, 0, el.size - 1)].astype(np.int64)
+    else:
+        first = last = np.zeros(len(p), np.int64)
+    gap = ((last - first) & 0xffffffff) // np.maximum(l - 1, 1)
+    d = np.where(l < 2, 3, np.where(gap < 4, 0, np.where(gap < 32, 1, np.where(gap < 256, 2, 3))))
+    log2 = lambda x: np.frexp(np.maximum(x, 1).astype(np.float64))[1].astype(np.int64) - 1  # exact floor(log2)
+    ls = np.where(s > 0, np.minimum(15, log2(s)), 0)
+    lr = np.where(s > 0, np.minimum(15, log2(l // np.maximum(s, 1))), 15)
+    return (d << 8) | (ls << 4) | lr
+
+
 def _pairs(pairs: torch.Tensor) -> int:
     if not pairs.is_cuda or pairs.dtype not in (torch.int32, torch.uint32) or not pairs.is_contiguous() or \
             pairs.dim() != 2 or pairs.shape[1] != 2:

@@ -79,6 +79,21 @@ def test_batch_arguments_and_table_layout_on_host():
     assert api.batch_bucket(1, 1) == (3 << 8) | (0 << 4) | 0
     with pytest.raises(ValueError):
         api._table(bytes(256))
+    # the vectorised form over a host collection agrees with the scalar one
+    rng = np.random.default_rng(1)
+    sizes = rng.integers(0, 900, 300)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    el = np.concatenate([np.sort(rng.choice(int(rng.choice([1 << 10, 1 << 16, 1 << 26])), size=int(n), replace=False))
+                         for n in sizes]).astype(np.uint32)
+    pairs = rng.integers(0, 300, (3000, 2)).astype(np.uint32)
+    want = []
+    for a, b in pairs:
+        na, nb = off[a + 1] - off[a], off[b + 1] - off[b]
+        big = a if na >= nb else b
+        n = off[big + 1] - off[big]
+        want.append(api.batch_bucket(int(na), int(nb), int(el[off[big]]) if n else 0,
+                                     int(el[off[big + 1] - 1]) if n else 0))
+    np.testing.assert_array_equal(api.batch_buckets(el, off, pairs), want)
 
 
 def test_dense_invalid_arguments_rejected_on_host():
