@@ -406,8 +406,9 @@ def run_ours(args, rank: int, world: int):
                "ms_per_step": e_step, "steps": e_steps,
                "host_buffers": "pinned: the caller's sets and result buffer, pinned before the timed region"}
         assert ce == c
-        # the same call from pageable host memory: the copies stage through
-        # the driver's buffers and no longer overlap the kernels
+        # the same call from pageable host memory: the library stages the
+        # inputs through its pinned buffers (host threads copy, the DMA engine
+        # moves the previous pieces up)
         pa = torch.from_numpy(a.view(np.int32))
         pb = torch.from_numpy(b.view(np.int32))
         pout = torch.empty(max(1, min(n_a, n_b)), dtype=torch.int32)

@@ -11,31 +11,112 @@
 // its own output region), its count and error word come back on the caller's
 // stream, and as soon as the host holds that count the range's elements are
 // copied back on a second copy stream to their final place in h_out.  The call
-// therefore costs about the host-to-device copy of the inputs (with pinned
-// host buffers; from pageable memory the copies are staged by the driver and
-// do not overlap).
+// therefore costs about the host-to-device copy of the inputs.  Pinned input
+// buffers are copied by the DMA engine directly; a pageable input is staged
+// through the context's pinned buffers: host threads copy 16 MiB pieces into
+// them while the DMA engine moves the previous pieces up (the driver's own
+// staging of pageable copies runs one piece at a time).
 //
-// The copy streams, the per-range events and the pinned words the counts and
-// error words land in belong to a si_host_ctx, created once (si_host_ctx_create)
-// and reused by every si_sisi_host_ctx call; si_sisi_host creates and destroys
-// one per call.
+// The copy streams, the per-range events, the pinned words the counts and
+// error words land in and the staging buffers belong to a si_host_ctx, created
+// once (si_host_ctx_create) and reused by every si_sisi_host_ctx call (one
+// call at a time per context); si_sisi_host creates and destroys one per call.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "si.h"
 #include "si_internal.h"
 
+namespace si {
+namespace {
+
+// Host threads that copy one buffer together (fork-join): the caller takes
+// the first slice, the workers the others.
+class CopyPool {
+public:
+    explicit CopyPool(unsigned threads) {
+        for (unsigned i = 1; i < threads; ++i) workers_.emplace_back([this, i] { loop(i); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+            ++gen_;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+    void copy(void* dst, const void* src, size_t n) {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            dst_ = static_cast<unsigned char*>(dst);
+            src_ = static_cast<const unsigned char*>(src);
+            n_ = n;
+            pending_ = static_cast<unsigned>(workers_.size());
+            ++gen_;
+        }
+        cv_.notify_all();
+        part(0);
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [this] { return pending_ == 0; });
+    }
+
+private:
+    void part(unsigned i) const {
+        const size_t parts = workers_.size() + 1;
+        const size_t step = ((n_ + parts - 1) / parts + 63) & ~size_t(63);
+        const size_t lo = std::min(n_, step * i), hi = std::min(n_, lo + step);
+        if (hi > lo) std::memcpy(dst_ + lo, src_ + lo, hi - lo);
+    }
+    void loop(unsigned i) {
+        uint64_t seen = 0;
+        for (;;) {
+            std::unique_lock<std::mutex> lk(m_);
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            if (stop_) return;
+            lk.unlock();
+            part(i);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    unsigned char* dst_ = nullptr;
+    const unsigned char* src_ = nullptr;
+    size_t n_ = 0;
+    unsigned pending_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
+}  // namespace
+}  // namespace si
+
 struct si_host_ctx {
     static constexpr uint32_t kMaxChunks = 64;
+    static constexpr uint32_t kStages = 4;                // staging buffers for pageable inputs
+    static constexpr size_t kStageBytes = size_t(16) << 20;
     int device = -1;
     cudaStream_t up = nullptr, down = nullptr;
     cudaEvent_t start = nullptr;
     cudaEvent_t landed[kMaxChunks] = {}, counted[kMaxChunks] = {};
     uint64_t* hcount = nullptr;  // pinned [kMaxChunks]
     uint32_t* herr = nullptr;    // pinned [kMaxChunks][4]: each range's workspace error header
+    // made at the first call with a pageable input
+    unsigned char* stage[kStages] = {};
+    cudaEvent_t stage_free[kStages] = {};  // the last copy up from the buffer has finished
+    uint32_t next_stage = 0;
+    si::CopyPool* pool = nullptr;
 };
 
 namespace si {
@@ -129,6 +210,52 @@ struct Drain {
     }
 };
 
+// True for memory the DMA engine can read directly (cudaHostAlloc'd or
+// registered); pageable memory is staged.
+bool host_pinned(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+si_status ensure_staging(si_host_ctx* ctx) {
+    if (ctx->pool) return SI_OK;
+    for (uint32_t k = 0; k < si_host_ctx::kStages; ++k) {
+        SI_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void**>(&ctx->stage[k]), si_host_ctx::kStageBytes,
+                                  cudaHostAllocDefault));
+        SI_CUDA_TRY(cudaEventCreateWithFlags(&ctx->stage_free[k], cudaEventDisableTiming));
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    ctx->pool = new CopyPool(std::min(8u, hw));
+    return SI_OK;
+}
+
+// bytes from host src to device dst on the context's up stream: directly from
+// pinned memory, else through the staging buffers (a buffer is refilled once
+// its previous copy up has finished; the host copy of one piece overlaps the
+// DMA of the pieces before it).
+si_status upload(si_host_ctx* ctx, void* dst, const void* src, size_t bytes, bool pinned) {
+    if (bytes == 0) return SI_OK;
+    if (pinned) {
+        SI_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->up));
+        return SI_OK;
+    }
+    for (size_t off = 0; off < bytes; off += si_host_ctx::kStageBytes) {
+        const size_t n = std::min(si_host_ctx::kStageBytes, bytes - off);
+        const uint32_t k = ctx->next_stage;
+        ctx->next_stage = (k + 1) % si_host_ctx::kStages;
+        SI_CUDA_TRY(cudaEventSynchronize(ctx->stage_free[k]));
+        ctx->pool->copy(ctx->stage[k], static_cast<const unsigned char*>(src) + off, n);
+        SI_CUDA_TRY(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, ctx->stage[k], n, cudaMemcpyHostToDevice,
+                                    ctx->up));
+        SI_CUDA_TRY(cudaEventRecord(ctx->stage_free[k], ctx->up));
+    }
+    return SI_OK;
+}
+
 }  // namespace
 }  // namespace si
 
@@ -174,6 +301,11 @@ extern "C" void si_host_ctx_destroy(si_host_ctx* c) {
     if (c->down) cudaStreamDestroy(c->down);
     if (c->hcount) cudaFreeHost(c->hcount);
     if (c->herr) cudaFreeHost(c->herr);
+    for (uint32_t k = 0; k < si_host_ctx::kStages; ++k) {
+        if (c->stage_free[k]) cudaEventDestroy(c->stage_free[k]);
+        if (c->stage[k]) cudaFreeHost(c->stage[k]);
+    }
+    delete c->pool;
     delete c;
 }
 
@@ -206,15 +338,31 @@ extern "C" si_status si_sisi_host_ctx(si_host_ctx* ctx, const uint32_t* hA, uint
     void* ws = w + L.off_ws;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
 
+    const bool pinned_a = si::host_pinned(hA), pinned_b = si::host_pinned(hB);
+    const bool staged = !pinned_a || !pinned_b;
+    if (staged) {
+        const si_status st = si::ensure_staging(ctx);
+        if (st != SI_OK) return st;
+    }
     si::Drain drain{ctx, s};
     // the copies up start after the caller's earlier work on its stream
     SI_CUDA_TRY(cudaEventRecord(ctx->start, s));
     SI_CUDA_TRY(cudaStreamWaitEvent(ctx->up, ctx->start, 0));
-    for (uint32_t i = 0; i < c.n; ++i) {
+    auto upload_range = [&](uint32_t i) -> si_status {
         const uint64_t a0 = c.a[i], na = c.a[i + 1] - a0, b0 = c.b[i], nb = c.b[i + 1] - b0;
-        if (na) SI_CUDA_TRY(cudaMemcpyAsync(dA + a0, hA + a0, na * 4, cudaMemcpyHostToDevice, ctx->up));
-        if (nb) SI_CUDA_TRY(cudaMemcpyAsync(dB + b0, hB + b0, nb * 4, cudaMemcpyHostToDevice, ctx->up));
+        si_status st = si::upload(ctx, dA + a0, hA + a0, na * 4, pinned_a);
+        if (st == SI_OK) st = si::upload(ctx, dB + b0, hB + b0, nb * 4, pinned_b);
+        if (st != SI_OK) return st;
         SI_CUDA_TRY(cudaEventRecord(ctx->landed[i], ctx->up));
+        return SI_OK;
+    };
+    // pinned inputs: every copy up is queued at once; staged ones are copied
+    // range by range, each range's kernels queued as soon as its copies are
+    if (!staged) {
+        for (uint32_t i = 0; i < c.n; ++i) {
+            const si_status st = upload_range(i);
+            if (st != SI_OK) return st;
+        }
     }
     std::vector<uint64_t> out_at(c.n + 1, 0);  // each range's output region on the device
     for (uint32_t i = 0; i < c.n; ++i)
@@ -235,6 +383,10 @@ extern "C" si_status si_sisi_host_ctx(si_host_ctx* ctx, const uint32_t* hA, uint
         return SI_OK;
     };
     for (uint32_t i = 0; i < c.n; ++i) {
+        if (staged) {
+            const si_status st = upload_range(i);
+            if (st != SI_OK) return st;
+        }
         const uint64_t a0 = c.a[i], na = c.a[i + 1] - a0, b0 = c.b[i], nb = c.b[i + 1] - b0;
         SI_CUDA_TRY(cudaStreamWaitEvent(s, ctx->landed[i], 0));
         const uint64_t cap = out_at[i + 1] - out_at[i];

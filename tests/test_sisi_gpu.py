@@ -218,6 +218,28 @@ def test_validate_sorted(cuda):
     assert api.validate_sorted(dev(np.zeros(1, np.uint32)))
 
 
+@pytest.mark.parametrize("pinned", [(False, False), (True, False), (False, True)])
+def test_intersect_host_staged_pageable_inputs(cuda, pinned):
+    """Pageable inputs larger than several 16 MiB staging buffers (ragged
+    tails), alone or beside a pinned one, reused on one context."""
+    import torch
+    from set_intersection_b200 import api, generate
+    a = generate.uniform(31, 9_000_001, 1 << 28)
+    b = generate.uniform(32, 7_654_321, 1 << 28)
+    want = oracle.set_intersection(a, b)
+    ha, hb = torch.from_numpy(a.view(np.int32)), torch.from_numpy(b.view(np.int32))
+    if pinned[0]:
+        ha = ha.pin_memory()
+    if pinned[1]:
+        hb = hb.pin_memory()
+    ctx = api.HostPair()
+    for _ in range(2):
+        c, got = api.intersect_host(ha, hb, "auto", ctx=ctx)
+        assert c == want.size
+        assert np.array_equal(got.numpy().view(np.uint32), want)
+    ctx.close()
+
+
 @pytest.mark.parametrize("chunks", [None, 1, 3, 8])
 @pytest.mark.parametrize("tech", ["auto", "ip", "bitmap"])
 def test_intersect_host_pipeline(cuda, tech, chunks):
