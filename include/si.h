@@ -104,7 +104,9 @@ si_status si_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
  * or more, else 1; at most 64) that are pipelined: one range's sets are copied
  * up while the previous range is intersected and the elements of earlier
  * ranges are copied down, so with pinned host buffers the call costs about the
- * host-to-device copy.  Pageable buffers work too, without the overlap.
+ * host-to-device copy.  A pageable input is staged through pinned buffers of
+ * the context: host threads copy 16 MiB pieces into them while the DMA engine
+ * moves the previous pieces up.
  *
  * d_workspace: device, 256-byte aligned, of si_sisi_host_workspace_size bytes
  * (it holds the device copies of both sets, the output and the per-range
@@ -122,7 +124,9 @@ si_status si_sisi_host(const uint32_t* hA, uint64_t nA, const uint32_t* hB, uint
  * per call; a caller that intersects many pairs creates one
  * (si_host_ctx_create, on the device that is current then) and passes it to
  * every si_sisi_host_ctx call on that device, which then creates, allocates
- * and frees nothing.  Calls sharing a context must not overlap (one host
+ * and frees nothing (the staging buffers for pageable inputs, 64 MiB of pinned
+ * memory and a pool of up to 8 copy threads, are made at the first call that
+ * needs them and kept).  Calls sharing a context must not overlap (one host
  * thread at a time).  Errors recorded on the device by any range are reported
  * (the first one); a set that descends across a range boundary is reported as
  * SI_ERR_INVALID_INPUT before anything is launched. */

@@ -253,11 +253,14 @@ __device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B
         const uint32_t cA = lastA <= m ? la : ring_upper(ra, oa, la, m);
         const uint32_t cB = lastB <= m ? lb : ring_upper(rb, ob, lb, m);
         // merge path over the round's cA + cB (<= 512) final elements: lane l
-        // takes merged positions [16 l, 16 l + 16); ties take the A element
-        // first, and an A element equal to the B element after it is a match
+        // takes merged positions [st l, st l + st), st = ceil(total / 32) (a
+        // warp-uniform trip count, so no lane idles on short rounds); ties take
+        // the A element first, and an A element equal to the B element after
+        // it is a match
         {
             const uint32_t tot = cA + cB;
-            const uint32_t d = min(16u * lane, tot), dend = min(d + 16u, tot);
+            const uint32_t st = (tot + 31) / 32;
+            const uint32_t d = min(st * lane, tot), dend = min(d + st, tot);
             // a = A elements among the first d merged: the first a in
             // [max(0, d - cB), min(d, cA)] with A[a] > B[d - 1 - a]
             uint32_t lo = d > cB ? d - cB : 0u, hi = min(d, cA);
@@ -270,8 +273,8 @@ __device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B
             uint32_t a = lo, b = d - lo;
             uint32_t va = ra[(oa + a) & kRingMask], vb = rb[(ob + b) & kRingMask];
             // branch-free steps; a value read past cA or cB is never used
-#pragma unroll
-            for (uint32_t x = 0; x < 16; ++x) {
+#pragma unroll 4
+            for (uint32_t x = 0; x < st; ++x) {
                 if (d + x < dend) {
                     const bool aok = a < cA, bok = b < cB;
                     const bool takeA = aok && (!bok || va <= vb);
@@ -401,12 +404,20 @@ __device__ __forceinline__ void chunk_hash_insert(uint32_t* tab, const uint4& g0
         const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
         left[q] = old != kHashEmpty && old != v[q];
     }
+    // the lanes' retries advance together, one slot per element and trip
+    bool any = false;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        while (left[q]) {
-            h[q] = (h[q] + 1) & (kHashSlots - 1);
-            const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
-            left[q] = old != kHashEmpty && old != v[q];
+    for (int q = 0; q < 8; ++q) any |= left[q];
+    while (__any_sync(kFullMask, any)) {
+        any = false;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (left[q]) {
+                h[q] = (h[q] + 1) & (kHashSlots - 1);
+                const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
+                left[q] = old != kHashEmpty && old != v[q];
+                any |= left[q];
+            }
         }
     }
 }
@@ -426,13 +437,20 @@ __device__ __forceinline__ uint32_t chunk_hash_probe(const uint32_t* tab, const 
         c += on && t == v[q];
         left[q] = on && t != v[q] && t != kHashEmpty;
     }
+    bool any = false;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        while (left[q]) {
-            h[q] = (h[q] + 1) & (kHashSlots - 1);
-            const uint32_t t = tab[h[q]];
-            c += t == v[q];
-            left[q] = t != v[q] && t != kHashEmpty;
+    for (int q = 0; q < 8; ++q) any |= left[q];
+    while (__any_sync(kFullMask, any)) {
+        any = false;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (left[q]) {
+                h[q] = (h[q] + 1) & (kHashSlots - 1);
+                const uint32_t t = tab[h[q]];
+                c += t == v[q];
+                left[q] = t != v[q] && t != kHashEmpty;
+                any |= left[q];
+            }
         }
     }
     return c;
