@@ -404,20 +404,12 @@ __device__ __forceinline__ void chunk_hash_insert(uint32_t* tab, const uint4& g0
         const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
         left[q] = old != kHashEmpty && old != v[q];
     }
-    // the lanes' retries advance together, one slot per element and trip
-    bool any = false;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) any |= left[q];
-    while (__any_sync(kFullMask, any)) {
-        any = false;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            if (left[q]) {
-                h[q] = (h[q] + 1) & (kHashSlots - 1);
-                const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
-                left[q] = old != kHashEmpty && old != v[q];
-                any |= left[q];
-            }
+    for (int q = 0; q < 8; ++q) {
+        while (left[q]) {
+            h[q] = (h[q] + 1) & (kHashSlots - 1);
+            const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
+            left[q] = old != kHashEmpty && old != v[q];
         }
     }
 }
@@ -437,20 +429,13 @@ __device__ __forceinline__ uint32_t chunk_hash_probe(const uint32_t* tab, const 
         c += on && t == v[q];
         left[q] = on && t != v[q] && t != kHashEmpty;
     }
-    bool any = false;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) any |= left[q];
-    while (__any_sync(kFullMask, any)) {
-        any = false;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            if (left[q]) {
-                h[q] = (h[q] + 1) & (kHashSlots - 1);
-                const uint32_t t = tab[h[q]];
-                c += t == v[q];
-                left[q] = t != v[q] && t != kHashEmpty;
-                any |= left[q];
-            }
+    for (int q = 0; q < 8; ++q) {
+        while (left[q]) {
+            h[q] = (h[q] + 1) & (kHashSlots - 1);
+            const uint32_t t = tab[h[q]];
+            c += t == v[q];
+            left[q] = t != v[q] && t != kHashEmpty;
         }
     }
     return c;
