@@ -42,6 +42,7 @@
 #include <algorithm>
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
+#include <mutex>
 #include <vector>
 
 #include "si_device.cuh"
@@ -206,16 +207,19 @@ __device__ __forceinline__ void store_block(uint32_t* ring, uint64_t blk, int la
     for (int t = 0; t < kVT; ++t) ring[s0 + lane + 32u * t] = r[t];
 }
 
-// Number of window elements w[0 .. len) (ring positions from o) that are <= v.
-__device__ __forceinline__ uint32_t ring_upper(const uint32_t* ring, uint32_t o, uint32_t len, uint32_t v) {
-    uint32_t lo = 0, n = len;
-    while (n > 0) {
-        const uint32_t half = n >> 1;
-        const bool c = ring[(o + lo + half) & kRingMask] <= v;
-        lo = c ? lo + half + 1 : lo;
-        n = c ? n - half - 1 : half;
-    }
-    return lo;
+// Number of window elements w[0 .. len) (ring positions from o) that are <= v,
+// warp-cooperative, for a sorted window of len <= 256: lane l
+// tests element 8 l, then the first eight lanes the elements of the one group
+// of eight the answer ends in (two shared loads and two ballots per lane).
+// Every lane gets the result.
+__device__ __forceinline__ uint32_t ring_count_le(const uint32_t* ring, uint32_t o, uint32_t len, uint32_t v,
+                                                  uint32_t lane) {
+    const uint32_t i1 = 8 * lane;
+    const uint32_t k = __popc(__ballot_sync(kFullMask, i1 < len && ring[(o + i1) & kRingMask] <= v));
+    if (k == 0) return 0;
+    const uint32_t i2 = 8 * (k - 1) + (lane & 7);
+    const bool c2 = lane < 8 && i2 < len && ring[(o + i2) & kRingMask] <= v;
+    return 8 * (k - 1) + __popc(__ballot_sync(kFullMask, c2));
 }
 
 // MERGE: |A ∩ B| by streaming both sets through the warp's rings: A's at
@@ -250,8 +254,8 @@ __device__ uint32_t merge_pair(const uint32_t* A, uint64_t na, const uint32_t* B
         const uint32_t lastA = ra[(oa + la - 1) & kRingMask], lastB = rb[(ob + lb - 1) & kRingMask];
         const uint32_t m = min(lastA, lastB);
         // the elements of both windows up to m are final this round
-        const uint32_t cA = lastA <= m ? la : ring_upper(ra, oa, la, m);
-        const uint32_t cB = lastB <= m ? lb : ring_upper(rb, ob, lb, m);
+        const uint32_t cA = lastA <= m ? la : ring_count_le(ra, oa, la, m, lane);
+        const uint32_t cB = lastB <= m ? lb : ring_count_le(rb, ob, lb, m, lane);
         // merge path over the round's cA + cB (<= 512) final elements: lane l
         // takes merged positions [st l, st l + st), st = ceil(total / 32) (a
         // warp-uniform trip count, so no lane idles on short rounds); ties take
@@ -653,6 +657,32 @@ TechTable default_table() {
     return T;
 }
 
+// Resident CTAs per SM of the two batch kernels on the current device (the
+// stream kernel's shared-memory attribute is set per device, once).
+struct BatchOccupancy {
+    int search = 0, stream = 0;
+};
+BatchOccupancy batch_occupancy() {
+    constexpr int kMaxDevices = 64;
+    static BatchOccupancy cached[kMaxDevices];
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return {};
+    std::lock_guard<std::mutex> lk(mu);
+    BatchOccupancy& o = cached[dev];
+    if (o.search == 0 || o.stream == 0) {
+        int a = 0, b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, batch_kernel<false>, kBThreads, 0) != cudaSuccess ||
+            cudaFuncSetAttribute(batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBSmem) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, batch_kernel<true>, kBThreads, kBSmem) != cudaSuccess)
+            return {};
+        o.search = a;
+        o.stream = b;
+    }
+    return o;
+}
+
 si_status batch_launch(const uint32_t* d_elements, const uint64_t* d_offsets, uint32_t k, const uint32_t* d_pairs,
                        uint64_t npairs, const TechTable& table, int forced, const uint32_t* d_subset,
                        uint64_t nsubset, uint32_t* d_counts, void* ws, size_t ws_bytes, cudaStream_t stream) {
@@ -686,19 +716,8 @@ si_status batch_launch(const uint32_t* d_elements, const uint64_t* d_offsets, ui
         SI_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w + L.off_cub, tmp, keys_in, keys, static_cast<int>(npairs), 0, 64,
                                                    stream));
     }
-    static const int search_per_sm = [] {
-        int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<false>, kBThreads, 0) != cudaSuccess) n = 0;
-        return n;
-    }();
-    static const int stream_per_sm = [] {
-        int n = 0;
-        if (cudaFuncSetAttribute(batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBSmem) !=
-                cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<true>, kBThreads, kBSmem) != cudaSuccess)
-            n = 0;
-        return n;
-    }();
+    const BatchOccupancy occ = batch_occupancy();
+    const int search_per_sm = occ.search, stream_per_sm = occ.stream;
     if (search_per_sm == 0 || stream_per_sm == 0) return cuda_fail(cudaGetLastError(), "batch_kernel attributes");
     // the subset of the tuner runs in its technique's kernel; the whole queue
     // in both, one part each (no stream part when every pair merges or searches)
