@@ -45,10 +45,11 @@ def test_random_pools(cuda, tech, k, n_min, n_max, universe, npairs, seed):
     np.testing.assert_array_equal(count(collection(el, off, universe - 1), pairs, tech), want)
 
 
-@pytest.mark.parametrize("tech", TECHS)
+@pytest.mark.parametrize("tech", TECHS + [f"code{c}" for c in CODES])
 def test_edge_pairs(cuda, tech):
     """Empty sets, a set with itself, subsets, disjoint value ranges, extreme
-    size ratios, the values 0 and 0xffffffff, windows that end on equal values."""
+    size ratios, the values 0 and 0xffffffff, windows that end on equal values;
+    the five techniques by name, and each of the six codes through a table."""
     top = np.uint32(0xffffffff)
     rng = np.random.default_rng(5)
     big = np.sort(rng.choice(1 << 24, size=200000, replace=False)).astype(np.uint32)
@@ -65,7 +66,9 @@ def test_edge_pairs(cuda, tech):
     k = ds.cardinality
     pairs = np.array([(a, b) for a in range(k) for b in range(k)], np.uint32)
     want = oracle.pairs(ds.elements, ds.offsets, k, pairs)
-    np.testing.assert_array_equal(count(collection(ds.elements, ds.offsets, ds.universe), pairs, tech), want)
+    table = bytes([int(tech[4:])]) * 1024 if tech.startswith("code") else None
+    got = count(collection(ds.elements, ds.offsets, ds.universe), pairs, "auto" if table else tech, table)
+    np.testing.assert_array_equal(got, want)
 
 
 def mixed_pool(seed):
