@@ -19,13 +19,14 @@
 //      MERGE (ip): the warp streams both sets through a shared-memory ring of
 //        two 256-element blocks per set; every round finalises the elements up
 //        to the smaller of the two window maxima and merges them along the
-//        merge path (each lane 16 merged positions after a split search, as
-//        the reference's intersectPath splits a partition, src/ip.cu:207-245),
-//        then slides; the next block of each set is prefetched into registers
-//        a round ahead.
+//        merge path (each lane an equal share of the merged positions after a
+//        split search, as the reference's intersectPath splits a partition,
+//        src/ip.cu:207-245), then slides; the next block of each set is
+//        prefetched into registers a round ahead.
 //      SEARCH (obs): the warp takes the smaller set 256 elements at a time,
-//        narrows the window of the larger set that can hold them (two binary
-//        searches), then every lane runs 8 interleaved binary searches in it.
+//        bounds the window of the larger set that can hold them, caches 256
+//        samples of a long window in shared memory, and every lane runs 8
+//        interleaved binary searches in the gaps between samples.
 //      HASH (hi, windows of 1024 or 512 elements): the smaller set S is cut
 //        into windows of consecutive elements; each window goes into the
 //        warp's 2048-slot open-addressing table (load <= 1/2 or 1/4) and the
@@ -327,9 +328,21 @@ __device__ uint32_t search_pair(const uint32_t* S, uint64_t ns, const uint32_t* 
     uint64_t from = 0;  // the windows advance monotonically
     for (uint64_t base = 0; base < ns; base += kW) {
         const uint64_t last_i = min(base + kW, ns) - 1;
-        const uint32_t v0 = __ldg(S + base), v1 = __ldg(S + last_i);
-        const uint64_t lo = warp_first_true(from, nl, [&](uint64_t i) { return __ldg(L + i) >= v0; });
-        const uint64_t hi = warp_first_true(lo, nl, [&](uint64_t i) { return __ldg(L + i) > v1; });
+        // a smaller set of one block searches all of L (its samples bound the
+        // gaps as well as a narrowed window would, without the two searches)
+        // later blocks start where the previous one's window ended (the L
+        // elements between are below this block's first value: harmless)
+        uint64_t lo = 0, hi = nl;
+        if (ns > kW) {
+            const uint32_t v1 = __ldg(S + last_i);
+            if (base == 0) {
+                const uint32_t v0 = __ldg(S);
+                lo = warp_first_true(0, nl, [&](uint64_t i) { return __ldg(L + i) >= v0; });
+            } else {
+                lo = from;
+            }
+            hi = warp_first_true(lo, nl, [&](uint64_t i) { return __ldg(L + i) > v1; });
+        }
         from = hi;
         if (lo >= hi) continue;
         const uint64_t W = hi - lo;
@@ -367,23 +380,50 @@ __device__ uint32_t search_pair(const uint32_t* S, uint64_t ns, const uint32_t* 
             }
             __syncwarp();  // the samples are read before the next block writes them
         }
-        // interleaved searches for the last element <= v: kVT independent load chains per lane
-        bool more = true;
-        while (more) {
-            more = false;
+        // interleaved searches for the last element <= v: kVT independent load
+        // chains per lane, in 32-bit offsets from lo when the window allows
+        if (W < (uint64_t(1) << 32)) {
+            const uint32_t* Lw = L + lo;
+            uint32_t o32[kVT], n32[kVT];
 #pragma unroll
             for (int t = 0; t < kVT; ++t) {
-                if (len[t] > 1) {
-                    const uint64_t half = len[t] >> 1;
-                    const bool c = __ldg(L + pos[t] + half) <= v[t];
-                    pos[t] = c ? pos[t] + half : pos[t];
-                    len[t] = c ? len[t] - half : half;
-                    more |= len[t] > 1;
+                o32[t] = static_cast<uint32_t>(pos[t] - lo);
+                n32[t] = static_cast<uint32_t>(len[t]);
+            }
+            bool more = true;
+            while (more) {
+                more = false;
+#pragma unroll
+                for (int t = 0; t < kVT; ++t) {
+                    if (n32[t] > 1) {
+                        const uint32_t half = n32[t] >> 1;
+                        const bool c = __ldg(Lw + o32[t] + half) <= v[t];
+                        o32[t] = c ? o32[t] + half : o32[t];
+                        n32[t] = c ? n32[t] - half : half;
+                        more |= n32[t] > 1;
+                    }
                 }
             }
-        }
 #pragma unroll
-        for (int t = 0; t < kVT; ++t) hits += (len[t] == 1 && __ldg(L + pos[t]) == v[t]) ? 1u : 0u;
+            for (int t = 0; t < kVT; ++t) hits += (n32[t] == 1 && __ldg(Lw + o32[t]) == v[t]) ? 1u : 0u;
+        } else {
+            bool more = true;
+            while (more) {
+                more = false;
+#pragma unroll
+                for (int t = 0; t < kVT; ++t) {
+                    if (len[t] > 1) {
+                        const uint64_t half = len[t] >> 1;
+                        const bool c = __ldg(L + pos[t] + half) <= v[t];
+                        pos[t] = c ? pos[t] + half : pos[t];
+                        len[t] = c ? len[t] - half : half;
+                        more |= len[t] > 1;
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < kVT; ++t) hits += (len[t] == 1 && __ldg(L + pos[t]) == v[t]) ? 1u : 0u;
+        }
     }
     return __reduce_add_sync(kFullMask, hits);
 }
