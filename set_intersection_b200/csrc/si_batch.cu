@@ -390,16 +390,31 @@ __device__ uint32_t search_pair(const uint32_t* S, uint64_t ns, const uint32_t* 
                 o32[t] = static_cast<uint32_t>(pos[t] - lo);
                 n32[t] = static_cast<uint32_t>(len[t]);
             }
+            // 4-ary steps (three independent loads, a quarter of the gap
+            // left) while the gap allows, then binary: half the dependent
+            // load rounds of a binary search
             bool more = true;
             while (more) {
                 more = false;
 #pragma unroll
                 for (int t = 0; t < kVT; ++t) {
-                    if (n32[t] > 1) {
-                        const uint32_t half = n32[t] >> 1;
+                    const uint32_t n = n32[t];
+                    if (n >= 4) {
+                        const uint32_t q1 = n >> 2, q2 = n >> 1, q3 = q1 + q2;
+                        const uint32_t o = o32[t];
+                        const bool c1 = __ldg(Lw + o + q1) <= v[t];
+                        const bool c2 = __ldg(Lw + o + q2) <= v[t];
+                        const bool c3 = __ldg(Lw + o + q3) <= v[t];
+                        const uint32_t lo_q = c3 ? q3 : c2 ? q2 : c1 ? q1 : 0u;
+                        const uint32_t hi_q = c3 ? n : c2 ? q3 : c1 ? q2 : q1;
+                        o32[t] = o + lo_q;
+                        n32[t] = hi_q - lo_q;
+                        more |= n32[t] > 1;
+                    } else if (n > 1) {
+                        const uint32_t half = n >> 1;
                         const bool c = __ldg(Lw + o32[t] + half) <= v[t];
                         o32[t] = c ? o32[t] + half : o32[t];
-                        n32[t] = c ? n32[t] - half : half;
+                        n32[t] = c ? n - half : half;
                         more |= n32[t] > 1;
                     }
                 }
