@@ -442,7 +442,7 @@ def run_ours(args, rank: int, world: int):
         engine = "obs" if min(n_a, n_b) * SKEW_RATIO < max(n_a, n_b) else "bitmap"
     kernel, launches = {
         "ip": ("ip_tile_kernel<merge path>", 3),
-        "hi": ("ip_tile_kernel<hash probe>", 3),
+        "hi": ("bh_stream_kernel", 2 if args.materialize else 1),
         "bitmap": ("bp_stream_kernel", 2 if args.materialize else 1),
         "obs": ("obs_search_kernel", 4 if args.materialize else 2),
     }[engine]

@@ -74,9 +74,10 @@ const char* si_last_error_string(void);
  * count; element output is this engine's addition, ordered as
  * std::set_intersection orders it.
  *
- * Techniques: IP merges and HI hashes the two sets tile by tile (value-pivot
- * tiles of <= 6144 elements per set for IP, <= 4096 for HI, whose smaller part
- * always fits its 8192-slot table; both sets streamed once); BITMAP streams
+ * Techniques: IP merges the two sets tile by tile (value-pivot tiles of <= 6144
+ * elements per set, both sets streamed once); HI streams them like BITMAP
+ * below, but each window of 512 elements of the smaller set goes into a
+ * warp-private hash table that the larger set's elements probe; BITMAP streams
  * the larger set in equal ranges, one warp per range, with the matching part
  * of the smaller set, through windows of 32768 values (two bitmaps per warp,
  * AND and popcount), and orders the output by a scan of the range counts,

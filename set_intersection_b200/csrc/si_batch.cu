@@ -444,91 +444,15 @@ __device__ uint32_t search_pair(const uint32_t* S, uint64_t ns, const uint32_t* 
 }
 
 // ---------------------------------------------------------------- HASH --
-constexpr uint32_t kHashSlots = 2048;          // per warp: 8 KiB
-constexpr uint32_t kHashEmpty = 0xffffffffu;   // the empty slot (that value is matched apart)
-
-__device__ __forceinline__ uint32_t hash_slot(uint32_t v) {  // Fibonacci hashing to 11 bits
-    return (v * 2654435761u) >> 21;
-}
-
-// Inserts the chunk's elements (8 per lane; repeated values are kept once).
-// A window holds at most kHashSlots / 2 distinct values, so every probe
-// sequence meets an empty slot.
-__device__ __forceinline__ void chunk_hash_insert(uint32_t* tab, const uint4& g0, const uint4& g1) {
-    uint32_t v[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w}, h[8];
-    bool left[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        h[q] = hash_slot(v[q]);
-        const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
-        left[q] = old != kHashEmpty && old != v[q];
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        while (left[q]) {
-            h[q] = (h[q] + 1) & (kHashSlots - 1);
-            const uint32_t old = atomicCAS(tab + h[q], kHashEmpty, v[q]);
-            left[q] = old != kHashEmpty && old != v[q];
-        }
-    }
-}
-
-// Matches of the chunk's elements whose bit is set in `valid` (bit q: g0's
-// component q, bit 4 + q: g1's).  No element is kHashEmpty.
-__device__ __forceinline__ uint32_t chunk_hash_probe(const uint32_t* tab, const uint4& g0, const uint4& g1,
-                                                     uint32_t valid) {
-    const uint32_t v[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
-    uint32_t h[8], c = 0;
-    bool left[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        h[q] = hash_slot(v[q]);
-        const uint32_t t = tab[h[q]];
-        const bool on = (valid >> q) & 1u;
-        c += on && t == v[q];
-        left[q] = on && t != v[q] && t != kHashEmpty;
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        while (left[q]) {
-            h[q] = (h[q] + 1) & (kHashSlots - 1);
-            const uint32_t t = tab[h[q]];
-            c += t == v[q];
-            left[q] = t != v[q] && t != kHashEmpty;
-        }
-    }
-    return c;
-}
-
-// Which of the chunk at s.pc this lane probes: stream positions in
-// [v0, s.v1) (the head and tail copies are not elements of their own) whose
-// value is <= hi (the later ones belong to the next window).
-__device__ __forceinline__ uint32_t probe_mask(const SetStream& s, const uint4& g0, const uint4& g1, uint32_t v0,
-                                               uint32_t hi, uint32_t lane) {
-    if ((s.pc != 0 || v0 == 0) && s.pc + kChunk <= s.v1 && s.last <= hi) return 0xffu;
-    uint32_t m = 0;
-#pragma unroll
-    for (uint32_t q = 0; q < 4; ++q) {
-        const uint32_t p0 = s.pc + 4 * lane + q, p1 = p0 + 128;
-        m |= (p0 >= v0 && p0 < s.v1 && comp(g0, q) <= hi ? 1u : 0u) << q;
-        m |= (p1 >= v0 && p1 < s.v1 && comp(g1, q) <= hi ? 1u : 0u) << (4 + q);
-    }
-    return m;
-}
-
-__device__ __forceinline__ bool stream_next(SetStream& s, uint32_t lane) {
-    return s.ph == 0 ? stream_advance<true>(s, lane) : stream_advance<false>(s, lane);
-}
-
 // HASH: |S ∩ L| (S the smaller set), windows of kWinChunks chunks of S.
 template <uint32_t kWinChunks>
 __device__ uint32_t hash_pair(const uint32_t* S, uint64_t ns, const uint32_t* L, uint64_t nl, uint32_t* tab,
                               uint32_t lane) {
-    static_assert(kWinChunks * kChunk <= kHashSlots / 2, "a window fills at most half of the table");
+    static_assert(kWinChunks * kChunk <= kWinHashSlots / 2, "a window fills at most half of the table");
     if (ns == 0 || nl == 0) return 0;
     // the value 2^32 - 1 marks empty slots: a match of it is counted here and
     // it leaves both sets (it can only be their last element)
-    const bool s_top = __ldg(S + ns - 1) == kHashEmpty, l_top = __ldg(L + nl - 1) == kHashEmpty;
+    const bool s_top = __ldg(S + ns - 1) == kWinHashEmpty, l_top = __ldg(L + nl - 1) == kWinHashEmpty;
     const uint32_t extra = s_top && l_top ? 1u : 0u;
     ns -= s_top;
     nl -= l_top;
@@ -544,8 +468,8 @@ __device__ uint32_t hash_pair(const uint32_t* S, uint64_t ns, const uint32_t* L,
     uint4* tab4 = reinterpret_cast<uint4*>(tab);
     uint32_t hits = 0;
     for (;;) {
-        for (uint32_t i = lane; i < kHashSlots / 4; i += 32)
-            tab4[i] = make_uint4(kHashEmpty, kHashEmpty, kHashEmpty, kHashEmpty);
+        for (uint32_t i = lane; i < kWinHashSlots / 4; i += 32)
+            tab4[i] = make_uint4(kWinHashEmpty, kWinHashEmpty, kWinHashEmpty, kWinHashEmpty);
         __syncwarp();
         // the window: the next kWinChunks chunks of S, up to its last value hi
         uint32_t hi = 0;
@@ -563,9 +487,9 @@ __device__ uint32_t hash_pair(const uint32_t* S, uint64_t ns, const uint32_t* L,
         bool more_l = true;
         for (;;) {
             if (sl.ph == 0)
-                hits += chunk_hash_probe(tab, sl.a0, sl.a1, probe_mask(sl, sl.a0, sl.a1, lv0, hi, lane));
+                hits += __popc(chunk_hash_probe(tab, sl.a0, sl.a1, probe_mask(sl, sl.a0, sl.a1, lv0, hi, lane)));
             else
-                hits += chunk_hash_probe(tab, sl.b0, sl.b1, probe_mask(sl, sl.b0, sl.b1, lv0, hi, lane));
+                hits += __popc(chunk_hash_probe(tab, sl.b0, sl.b1, probe_mask(sl, sl.b0, sl.b1, lv0, hi, lane)));
             if (sl.last > hi) break;
             more_l = stream_next(sl, lane);
             if (!more_l) break;

@@ -59,9 +59,12 @@ si_status pivot_split(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint6
                       uint64_t* split_a, uint64_t* split_b, uint32_t* samples_a, uint32_t* samples_b,
                       uint64_t* zero, uint64_t nzero, uint64_t* d_count, cudaStream_t stream);
 size_t pivot_samples_bytes(uint64_t nA, uint64_t nB, uint64_t S);
+// The stream engine of si_sisi_bitmap.cu: window bitmaps (technique bitmap)
+// or, with hash set, window hash tables (technique hi) on the same ranges.
 size_t bm_workspace_size(uint64_t nA, uint64_t nB);
 si_status bm_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
-                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream);
+                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream,
+                  bool hash = false);
 // SI_TECH_AUTO searches the smaller set in the larger (obs) when the sizes
 // differ by more than this factor.
 constexpr uint64_t kSkewRatio = 64;

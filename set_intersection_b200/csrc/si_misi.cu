@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kMisiThreads, misi_ctas_per_sm(kTech)) misi_pr
     __shared__ uint64_t s_item;
     __shared__ unsigned long long s_next;  // the next slice of the item's partner elements
     __shared__ uint32_t s_has_max;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     const uint32_t rows = p.nA + p.nB;
     const uint64_t n_items = p.items[rows];
 

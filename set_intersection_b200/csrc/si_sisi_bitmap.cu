@@ -26,6 +26,11 @@
 //      and the total count.  Launched as a programmatic dependent, so its
 //      launch overlaps the stream kernel's tail.
 //
+//  bh_stream_kernel  technique hi on the same ranges: Y in windows of 512
+//      elements goes into a warp-private 2048-slot hash table (load <= 1/4),
+//      the range's X elements up to the window's last value probe it; the
+//      same scratch, range scan and copy kernel as the bitmap stream.
+//
 //  pivot_sample_kernel + pivot_split_kernel  the intersect-path tiles' split
 //      (si_sisi_ip.cu): every S-th element of each set is a pivot; one warp
 //      per pivot finds its rank in the merged pivot order (a merge-path search
@@ -163,6 +168,45 @@ constexpr uint64_t kMinRange = 4096;            // X elements per warp, at least
 constexpr uint32_t kBmBytes = kWinWords * 4;    // one bitmap, aligned to its size in shared memory
 constexpr size_t kStSmem = size_t(kStWarps) * 2 * kBmBytes + kBmBytes;  // + the skew to a bitmap boundary
 
+// The last CTA of a stream kernel to finish turns the ranges' counts into
+// output offsets (exclusive prefix sums; 256 threads, a contiguous share of
+// the ranges each).
+__device__ __forceinline__ void last_cta_scan(const uint32_t* __restrict__ range_count,
+                                              uint64_t* __restrict__ range_off, uint64_t nRanges,
+                                              uint32_t* __restrict__ done_ctas) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ uint32_t s_last;
+    __shared__ uint64_t s_warp[kStWarps];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done_ctas, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const uint64_t per = (nRanges + kStBlock - 1) / kStBlock;
+    const uint64_t r0 = nRanges < threadIdx.x * per ? nRanges : threadIdx.x * per;
+    const uint64_t r1 = nRanges < r0 + per ? nRanges : r0 + per;
+    uint64_t sum = 0;
+    for (uint64_t r = r0; r < r1; ++r) sum += __ldcg(range_count + r);
+    uint64_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t n = __shfl_up_sync(kFullMask, incl, d);
+        if (static_cast<int>(lane) >= d) incl += n;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint64_t before = 0;
+    for (uint32_t w = 0; w < warp; ++w) before += s_warp[w];
+    uint64_t off = before + incl - sum;
+    for (uint64_t r = r0; r < r1; ++r) {
+        range_off[r] = off;
+        off += __ldcg(range_count + r);
+    }
+}
+
 // One warp per range r of X: X elements [r L, (r + 1) L) and the Y elements
 // from the first one not below X[r L] on.  Both streams pass through windows
 // of kWin values [a, a + kWin): each window's X and Y elements set bits in the
@@ -248,38 +292,116 @@ __global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bp_stream_kernel(
     if constexpr (!kOut) {
         if (lane == 0 && my_hits) atomicAdd(reinterpret_cast<unsigned long long*>(d_count), my_hits);
     } else {
-        // the last CTA to finish turns the ranges' counts into output offsets
-        __shared__ uint32_t s_last;
-        __shared__ uint64_t s_warp[kStWarps];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            s_last = atomicAdd(done_ctas, 1u) == gridDim.x - 1;
+        last_cta_scan(range_count, range_off, nRanges, done_ctas);
+    }
+}
+
+// ------------------------------------------------------------ hash stream --
+// Technique hi on the same ranges (the reference's hash intersection,
+// src/hi.cu:295-479, in windows): one warp per range r of X streams Y from its
+// first element not below X[r L] in windows of kHashWinChunks chunks; each
+// window goes into the warp's kWinHashSlots-slot table (load <= 1/4) and the
+// range's X elements up to the window's last value probe it.  Element output
+// as the bitmap stream's: hits in value order to scratch[range_y[r] ...].
+// The value 2^32 - 1 marks empty slots; it can only be the last element of X
+// and of Y, and a match of it is added at the end of the last range.
+constexpr uint32_t kHashWinChunks = 2;  // 512 elements of Y per window
+constexpr size_t kHashSmem = size_t(kStWarps) * kWinHashSlots * sizeof(uint32_t);
+static_assert(kHashWinChunks * kChunk <= kWinHashSlots / 2, "a window fills at most half of the table");
+
+template <bool kOut>
+__global__ void __launch_bounds__(kStBlock, kStCtasPerSm) bh_stream_kernel(
+    const uint32_t* __restrict__ X, uint64_t nX, const uint32_t* __restrict__ Y, uint64_t nY, uint64_t L,
+    uint64_t nRanges, uint32_t* __restrict__ range_count, uint64_t* __restrict__ range_y,
+    uint64_t* __restrict__ range_off, uint32_t* __restrict__ scratch, uint64_t* __restrict__ d_count,
+    uint32_t* __restrict__ done_ctas) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t* tab = smem + warp * kWinHashSlots;
+    uint4* tab4 = reinterpret_cast<uint4*>(tab);
+    const bool y_top = __ldg(Y + nY - 1) == kWinHashEmpty, x_top = __ldg(X + nX - 1) == kWinHashEmpty;
+    const uint64_t nYe = nY - (y_top ? 1 : 0);  // Y without 2^32 - 1
+    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * kStWarps;
+    uint64_t my_hits = 0;
+    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * kStWarps + warp; r < nRanges; r += nwarps) {
+        const uint64_t xs = r * L, xe = min(xs + L, nX);
+        const bool top_here = x_top && xe == nX;  // this range holds X's 2^32 - 1
+        const uint64_t xe_e = xe - (top_here ? 1 : 0);
+        uint32_t hits = 0;
+        uint64_t ys = nYe;
+        if (xe_e > xs && nYe > 0) {
+            const uint32_t vfirst = __ldg(X + xs);
+            ys = warp_first_true(0, nYe, [&](uint64_t i) { return __ldg(Y + i) >= vfirst; });
         }
-        __syncthreads();
-        if (s_last) {
-            __threadfence();
-            const uint64_t per = (nRanges + kStBlock - 1) / kStBlock;
-            const uint64_t r0 = nRanges < threadIdx.x * per ? nRanges : threadIdx.x * per;
-            const uint64_t r1 = nRanges < r0 + per ? nRanges : r0 + per;
-            uint64_t sum = 0;
-            for (uint64_t r = r0; r < r1; ++r) sum += __ldcg(range_count + r);
-            uint64_t incl = sum;
+        if (ys < nYe) {
+            SetStream sx, sy;
+            stream_init(sx, X, xs, xe_e, lane);
+            stream_init(sy, Y, ys, nYe, lane);
+            const uint32_t xv0 = sx.v1 - static_cast<uint32_t>(xe_e - xs);  // X's first stream position
+            uint32_t* dst = kOut ? scratch + ys : nullptr;
+            for (;;) {
+                for (uint32_t i = lane; i < kWinHashSlots / 4; i += 32)
+                    tab4[i] = make_uint4(kWinHashEmpty, kWinHashEmpty, kWinHashEmpty, kWinHashEmpty);
+                __syncwarp();
+                // the window: the next chunks of Y, up to its last value hi
+                uint32_t hi = 0;
+                bool more_y = true;
+                for (uint32_t c = 0; c < kHashWinChunks && more_y; ++c) {
+                    if (sy.ph == 0)
+                        chunk_hash_insert(tab, sy.a0, sy.a1);
+                    else
+                        chunk_hash_insert(tab, sy.b0, sy.b1);
+                    hi = sy.last;
+                    more_y = stream_next(sy, lane);
+                }
+                __syncwarp();
+                // the range's X elements up to hi probe it; a chunk reaching past hi stays
+                bool more_x = true;
+                for (;;) {
+                    const uint4 g0 = sx.ph == 0 ? sx.a0 : sx.b0, g1 = sx.ph == 0 ? sx.a1 : sx.b1;
+                    const uint32_t hit = chunk_hash_probe(tab, g0, g1, probe_mask(sx, g0, g1, xv0, hi, lane));
+                    if constexpr (kOut) {
+                        // in value order: the chunk's first half (g0, lane by lane), then its second
+                        const uint32_t c0 = __popc(hit & 0xfu), c1 = __popc(hit >> 4);
+                        const uint32_t i0 = warp_inclusive_scan(c0), t0 = __shfl_sync(kFullMask, i0, 31);
+                        const uint32_t i1 = warp_inclusive_scan(c1), t1 = __shfl_sync(kFullMask, i1, 31);
+                        uint32_t* o0 = dst + hits + i0 - c0;
+                        uint32_t* o1 = dst + hits + t0 + i1 - c1;
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint64_t n = __shfl_up_sync(kFullMask, incl, d);
-                if (static_cast<int>(lane) >= d) incl += n;
-            }
-            if (lane == 31) s_warp[warp] = incl;
-            __syncthreads();
-            uint64_t before = 0;
-            for (uint32_t w = 0; w < warp; ++w) before += s_warp[w];
-            uint64_t off = before + incl - sum;
-            for (uint64_t r = r0; r < r1; ++r) {
-                range_off[r] = off;
-                off += __ldcg(range_count + r);
+                        for (uint32_t q = 0; q < 4; ++q)
+                            if ((hit >> q) & 1u) *o0++ = comp(g0, q);
+#pragma unroll
+                        for (uint32_t q = 0; q < 4; ++q)
+                            if ((hit >> (4 + q)) & 1u) *o1++ = comp(g1, q);
+                        hits += t0 + t1;
+                    } else {
+                        hits += __reduce_add_sync(kFullMask, __popc(hit));
+                    }
+                    if (sx.last > hi) break;
+                    more_x = stream_next(sx, lane);
+                    if (!more_x) break;
+                }
+                if (!more_x || !more_y) break;
+                __syncwarp();  // the probes are done before the table is cleared
             }
         }
+        if (top_here && y_top) {  // 2^32 - 1 in both sets: the last hit of the last range
+            if (kOut && lane == 0) scratch[ys + hits] = kWinHashEmpty;
+            ++hits;
+        }
+        if constexpr (kOut) {
+            if (lane == 0) {
+                range_count[r] = hits;
+                range_y[r] = ys;
+            }
+        } else {
+            my_hits += hits;
+        }
+    }
+    if constexpr (!kOut) {
+        if (lane == 0 && my_hits) atomicAdd(reinterpret_cast<unsigned long long*>(d_count), my_hits);
+    } else {
+        last_cta_scan(range_count, range_off, nRanges, done_ctas);
     }
 }
 
@@ -413,7 +535,7 @@ size_t pivot_samples_bytes(uint64_t nA, uint64_t nB, uint64_t S) {
 size_t bm_workspace_size(uint64_t nA, uint64_t nB) { return make_bp_layout(nA, nB).total; }
 
 si_status bm_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
-                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream) {
+                  uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream, bool hash) {
     const BpLayout L = make_bp_layout(nA, nB);
     if (ws_bytes < (d_out ? L.total : L.total_count_only)) return SI_ERR_WORKSPACE_TOO_SMALL;
     if (std::max(nA, nB) >= kMaxStream) return SI_ERR_UNSUPPORTED;
@@ -435,19 +557,19 @@ si_status bm_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
         if (!d_out || nX == 0 || nY == 0) SI_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), stream));
     }
     if (nX == 0 || nY == 0) return SI_OK;
+    const size_t smem = hash ? kHashSmem : kStSmem;
     auto launch = [&](auto kernel) -> si_status {
-        SI_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kStSmem)));
+        SI_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(
             (L.nRanges + kStWarps - 1) / kStWarps, static_cast<uint64_t>(sm_count()) * kStCtasPerSm));
         PhaseTimer timer("sisi_tile", stream);
-        kernel<<<grid, kStBlock, kStSmem, stream>>>(X, nX, Y, nY, L.L, L.nRanges, range_count, range_y, range_off,
-                                                    scratch, d_count, reinterpret_cast<uint32_t*>(w + kDoneCtas));
-        SI_LAUNCH_CHECK("bp_stream_kernel");
+        kernel<<<grid, kStBlock, smem, stream>>>(X, nX, Y, nY, L.L, L.nRanges, range_count, range_y, range_off,
+                                                 scratch, d_count, reinterpret_cast<uint32_t*>(w + kDoneCtas));
+        SI_LAUNCH_CHECK(hash ? "bh_stream_kernel" : "bp_stream_kernel");
         return SI_OK;
     };
-    if (!d_out) return launch(bp_stream_kernel<false>);
-    si_status st = launch(bp_stream_kernel<true>);
+    if (!d_out) return launch(hash ? bh_stream_kernel<false> : bp_stream_kernel<false>);
+    si_status st = launch(hash ? bh_stream_kernel<true> : bp_stream_kernel<true>);
     if (st != SI_OK) return st;
     PhaseTimer timer("sisi_copy", stream);
     const unsigned grid = static_cast<unsigned>(

@@ -24,8 +24,8 @@
 //    look-back over tile aggregates (single pass); count-only mode instead
 //    accumulates tile counts into 256 spread partial sums.
 //
-// Technique bitmap (and auto for pairs of similar size) shares the pivot
-// split and runs its own engine (si_sisi_bitmap.cu).
+// Techniques bitmap (and auto for pairs of similar size) and hi run the stream
+// engine of si_sisi_bitmap.cu, which also holds the pivot split.
 #include <algorithm>
 
 #include "si_device.cuh"
@@ -34,11 +34,7 @@
 namespace si {
 namespace {
 
-// Pivot (sample) stride: a tile holds at most this many elements of each set.
-// The hash probe's tiles are shorter, so that the smaller part of every tile
-// fills at most half of its table.
-__host__ __device__ constexpr uint32_t tile_stride(int inner) { return inner == 2 ? 4096u : 6144u; }
-constexpr uint32_t kS = tile_stride(0);
+constexpr uint32_t kS = 6144;  // pivot (sample) stride: a tile holds at most this many elements of each set
 constexpr int kPartials = 256;
 
 constexpr uint64_t kFlagAgg = 1ull << 62;
@@ -103,25 +99,12 @@ constexpr int kCtasPerSm = 2;
 constexpr int kSlots = 8;
 constexpr int kOutQ = 16;                    // output descriptors in flight
 constexpr int kGroup = 4;                    // consecutive tiles per scheduling unit (one look-back each)
-constexpr uint32_t kInRing = 14336;          // u32: 56 KiB (the merge path adds 16 KiB: 72 KiB)
-constexpr uint32_t kHashSlots = 8192;        // open-addressing table (32 KiB): load factor <= 1/2
-// Output ring: a power of two of words holding at least one tile's matches.
-__host__ __device__ constexpr uint32_t out_ring_words(int inner) { return inner == 2 ? 4096u : 8192u; }
-// Shared memory: input ring, output ring, and for the hash probe its table.
-// The merge path needs no table, so its input ring is longer (about three
-// average tiles instead of two); the hash probe's shorter tiles need half the
-// output ring.  Both come to 106.5 KiB: two CTAs per SM.
-__host__ __device__ constexpr uint32_t in_ring_words(int inner) {
-    return inner == 0 ? kInRing + 4096u : kInRing;
-}
-__host__ __device__ constexpr size_t smem_bytes(int inner) {
-    return size_t(in_ring_words(inner) + out_ring_words(inner) + (inner == 2 ? kHashSlots : 0)) * sizeof(uint32_t);
-}
-static_assert((out_ring_words(0) & (out_ring_words(0) - 1)) == 0 && (out_ring_words(2) & (out_ring_words(2) - 1)) == 0,
-              "output ring is indexed modulo its size");
-static_assert(tile_stride(0) <= out_ring_words(0) && tile_stride(2) <= out_ring_words(2),
-              "one tile's matches must fit the output ring");
-static_assert(tile_stride(2) <= kHashSlots / 2, "a tile's smaller part fills at most half of the hash table");
+constexpr uint32_t kInRing = 18432;          // u32: 72 KiB, about three average tiles
+constexpr uint32_t kOutRing = 8192;          // u32: 32 KiB, a power of two
+// Shared memory: input ring and output ring, 104 KiB: two CTAs per SM.
+constexpr size_t kTileSmem = size_t(kInRing + kOutRing) * sizeof(uint32_t);
+static_assert((kOutRing & (kOutRing - 1)) == 0, "output ring is indexed modulo its size");
+static_assert(kS <= kOutRing, "one tile's matches must fit the output ring");
 constexpr uint32_t kEndTile = 0xffffffffu;
 constexpr uint32_t kConsumerBar = 1;  // named barrier id of the consumer warps
 
@@ -205,7 +188,8 @@ __device__ __forceinline__ uint64_t look_back(uint64_t* status, uint64_t t, uint
 // owns as a bit mask over a contiguous run of one staged set: the matched
 // values are src[start + x] for every set bit x, in ascending order, and the
 // runs of consecutive threads are consecutive.
-// (kBitmapProbe selects the separate bitmap engine of si_sisi_bitmap.cu.)
+// (kBitmapProbe and kHashProbe select the stream engine of si_sisi_bitmap.cu,
+// with window bitmaps or window hash tables.)
 enum Inner { kMergePath = 0, kBitmapProbe = 1, kHashProbe = 2 };
 
 struct ThreadMatches {
@@ -267,67 +251,7 @@ __device__ __forceinline__ ThreadMatches merge_inner(const uint32_t* sA, int na,
     return {sA, i0, mask};
 }
 
-// Hash probe (the reference's hi, src/hi.cu:295-479, restricted to one tile):
-// the smaller set part is inserted into an open-addressing table in shared
-// memory (multiplicative hash, linear probing, load factor <= 1/2), the other
-// part probes it.  Tiles hold at most 4096 elements of each set, so every
-// tile's smaller part fits the 8192-slot (32 KiB) table: no tile falls back
-// to the merge path.
-// 0xffffffff marks an empty slot; the value 0xffffffff itself
-// can only be the last element of a part and is carried by a flag instead.
-// The table is cleared at the start of every hash tile, once every consumer
-// thread is past the previous tile's probes (the element-output path's
-// per-tile scan barrier orders that already; count-only needs one more).
-constexpr uint32_t kHashEmpty = 0xffffffffu;
-// The whole table is used for every tile: its load stays <= 1/2 and is about
-// 1/4 on average, which keeps probe sequences short (a table sized to each
-// tile's smaller part, load ~1/2, measured 10 % slower on the 2^28 pair).
-__device__ __forceinline__ uint32_t hash_slot(uint32_t v) { return (v * 0x9e3779b1u) >> (32 - 13); }
-static_assert(kHashSlots == (1u << 13), "hash_slot yields 13 bits");
-
-__device__ __forceinline__ ThreadMatches hash_inner(const uint32_t* sA, int na, const uint32_t* sB, int nb, int tid,
-                                                    uint32_t* table, uint32_t* s_has_max, bool need_barrier) {
-    if (need_barrier) named_barrier(kConsumerBar, kConsumers);
-    const bool buildA = na <= nb;
-    const uint32_t* X = buildA ? sA : sB;
-    const uint32_t* Y = buildA ? sB : sA;
-    const int nx = buildA ? na : nb, ny = buildA ? nb : na;
-    constexpr uint32_t mask = kHashSlots - 1;
-    uint4* t4 = reinterpret_cast<uint4*>(table);
-    for (uint32_t w = tid; w <= mask / 4; w += kConsumers)
-        t4[w] = make_uint4(kHashEmpty, kHashEmpty, kHashEmpty, kHashEmpty);
-    if (tid == 0) *s_has_max = 0u;
-    named_barrier(kConsumerBar, kConsumers);
-    for (int e = tid; e < nx; e += kConsumers) {
-        const uint32_t v = X[e];
-        if (v == kHashEmpty) {
-            *s_has_max = 1u;
-            continue;
-        }
-        uint32_t h = hash_slot(v);
-        while (atomicCAS(table + h, kHashEmpty, v) != kHashEmpty) h = (h + 1) & mask;
-    }
-    named_barrier(kConsumerBar, kConsumers);
-    const uint32_t has_max = *s_has_max;
-    const int r = ((ny + kConsumers - 1) / kConsumers) | 1;
-    const int j0 = min(tid * r, ny), j1 = min(j0 + r, ny);
-    uint64_t mask64 = 0;
-    for (int e = j0; e < j1; ++e) {
-        const uint32_t v = Y[e];
-        bool hit;
-        if (v == kHashEmpty) {
-            hit = has_max != 0;
-        } else {
-            uint32_t h = hash_slot(v), t;
-            while ((t = table[h]) != v && t != kHashEmpty) h = (h + 1) & mask;
-            hit = t == v;
-        }
-        mask64 |= (hit ? 1ull : 0ull) << (e - j0);
-    }
-    return {Y, j0, mask64};
-}
-
-template <bool kOut, int kInner>
+template <bool kOut>
 __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     const uint32_t* __restrict__ A, uint64_t nA, const uint32_t* __restrict__ B, uint64_t nB,
     const uint64_t* __restrict__ split_a, const uint64_t* __restrict__ split_b, uint64_t nTiles,
@@ -335,11 +259,9 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     uint64_t* __restrict__ d_count) {
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* in_ring = smem;
-    constexpr uint32_t kRing = in_ring_words(kInner);
-    constexpr uint32_t kOutRing = out_ring_words(kInner);
-    constexpr uint64_t kTileMax = tile_stride(kInner);
+    constexpr uint32_t kRing = kInRing;
+    constexpr uint64_t kTileMax = kS;
     uint32_t* out_ring = smem + kRing;
-    uint32_t* table = smem + kRing + kOutRing;  // hash probe: the hash table
     __shared__ __align__(8) uint64_t full[kSlots], empty[kSlots], ofull[kOutQ], oempty[kOutQ];
     __shared__ __align__(8) uint64_t s_released_out;  // output ring: virtual offset written out so far
     __shared__ uint32_t s_otile[kOutQ], s_ocount[kOutQ];
@@ -347,7 +269,6 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     __shared__ InDesc in_desc[kSlots];
     __shared__ uint64_t s_in_end[kSlots];  // producer-private: ring end of the tile in each slot
     __shared__ uint32_t s_warp[2][kConsumerWarps];  // by tile parity: a warp may run one tile ahead
-    __shared__ uint32_t s_has_max;                  // hash probe: the table's part holds 0xffffffff
 
     uint32_t* err = reinterpret_cast<uint32_t*>(ws);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -536,21 +457,16 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
     for (;; ++k) {
         const uint32_t slot = k % kSlots;
         bool gave_up = !mbar_wait_bounded(&full[slot], (k / kSlots) & 1, err, 5, k);
-        // Consumers that meet at named barriers (element output, hash probe)
-        // give up together: a warp leaving alone would leave the others at a
-        // barrier it never reaches, which has no time limit.
-        if constexpr (kOut || kInner == kHashProbe) gave_up = named_barrier_or(kConsumerBar, kConsumers, gave_up);
+        // Consumers that meet at named barriers (element output) give up
+        // together: a warp leaving alone would leave the others at a barrier
+        // it never reaches, which has no time limit.
+        if constexpr (kOut) gave_up = named_barrier_or(kConsumerBar, kConsumers, gave_up);
         if (gave_up) break;
         const InDesc d = in_desc[slot];
         if (d.tile == kEndTile) break;
         const uint32_t* sA = in_ring + d.offA;
         const uint32_t* sB = in_ring + d.offB;
-        ThreadMatches tm;
-        if (kInner == kHashProbe && d.na > 0 && d.nb > 0) {
-            tm = hash_inner(sA, d.na, sB, d.nb, tid, table, &s_has_max, !kOut);
-        } else {
-            tm = merge_inner(sA, d.na, sB, d.nb, d.fast != 0, tid);
-        }
+        const ThreadMatches tm = merge_inner(sA, d.na, sB, d.nb, d.fast != 0, tid);
         const uint32_t cnt = static_cast<uint32_t>(__popcll(tm.mask));
 
         if constexpr (!kOut) {
@@ -628,13 +544,14 @@ __global__ void __launch_bounds__(kBlock, kCtasPerSm) ip_tile_kernel(
 }  // namespace
 
 size_t ip_workspace_size(uint64_t nA, uint64_t nB, int inner) {
-    return inner == kBitmapProbe ? bm_workspace_size(nA, nB) : make_layout(nA, nB, tile_stride(inner)).total;
+    return inner == kMergePath ? make_layout(nA, nB, kS).total : bm_workspace_size(nA, nB);
 }
 
 si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t* d_count,
                   uint32_t* d_out, uint64_t out_cap, void* ws, size_t ws_bytes, cudaStream_t stream, int inner) {
-    if (inner == kBitmapProbe) return bm_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, ws, ws_bytes, stream);
-    const uint64_t S = tile_stride(inner);
+    if (inner != kMergePath)
+        return bm_sisi(dA, nA, dB, nB, d_count, d_out, out_cap, ws, ws_bytes, stream, inner == kHashProbe);
+    const uint64_t S = kS;
     const Layout L = make_layout(nA, nB, S);
     if (ws_bytes < L.total) return SI_ERR_WORKSPACE_TOO_SMALL;
     if (L.nTiles > 0x7fffffffull) return SI_ERR_INVALID_ARGUMENT;
@@ -652,7 +569,7 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
 
     const uint64_t nGroups = (L.nTiles + kGroup - 1) / kGroup;
     auto launch = [&](auto kernel, uint32_t* out) -> si_status {
-        const size_t smem = smem_bytes(inner);
+        const size_t smem = kTileSmem;
         SI_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         int per_sm = 0;
         SI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem));
@@ -668,12 +585,7 @@ si_status ip_sisi(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t 
                                                 smem, stream));
         return SI_OK;
     };
-    si_status st;
-    if (inner == kHashProbe) {
-        st = d_out ? launch(ip_tile_kernel<true, kHashProbe>, d_out) : launch(ip_tile_kernel<false, kHashProbe>, nullptr);
-    } else {
-        st = d_out ? launch(ip_tile_kernel<true, kMergePath>, d_out) : launch(ip_tile_kernel<false, kMergePath>, nullptr);
-    }
+    const si_status st = d_out ? launch(ip_tile_kernel<true>, d_out) : launch(ip_tile_kernel<false>, nullptr);
     if (st != SI_OK) return st;
     SI_LAUNCH_CHECK("sisi_tile_kernel");
     return SI_OK;

@@ -1,7 +1,8 @@
 // si_stream.cuh -- a sorted set read by one warp as a stream of 256-element
-// chunks, and the window bitmaps built from such streams: the building blocks
-// of the single-pair bitmap engine (si_sisi_bitmap.cu) and of the batched
-// pairs' window techniques (si_batch.cu).
+// chunks, and the window bitmaps and window hash tables built from such
+// streams: the building blocks of the single-pair bitmap and hash engines
+// (si_sisi_bitmap.cu) and of the batched pairs' window techniques
+// (si_batch.cu).
 #pragma once
 
 #include <cstdint>
@@ -209,6 +210,86 @@ __device__ __forceinline__ uint32_t chunk_first_from(const uint4& g0, const uint
 
 __device__ __forceinline__ uint32_t stream_first_from(const SetStream& s, uint64_t e) {
     return s.ph == 0 ? chunk_first_from(s.a0, s.a1, e) : chunk_first_from(s.b0, s.b1, e);
+}
+
+// ------------------------------------------------------------ window hash --
+// A warp-private open-addressing table of a window of one stream's elements,
+// probed by the other stream's chunks.
+constexpr uint32_t kWinHashSlots = 2048;          // per warp: 8 KiB
+constexpr uint32_t kWinHashEmpty = 0xffffffffu;   // the empty slot (that value is matched apart)
+
+__device__ __forceinline__ uint32_t win_hash_slot(uint32_t v) {  // Fibonacci hashing to 11 bits
+    return (v * 2654435761u) >> 21;
+}
+
+// Inserts the chunk's elements (8 per lane; repeated values are kept once).
+// A window holds at most kWinHashSlots / 2 distinct values, so every probe
+// sequence meets an empty slot.
+__device__ __forceinline__ void chunk_hash_insert(uint32_t* tab, const uint4& g0, const uint4& g1) {
+    uint32_t v[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w}, h[8];
+    bool left[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        h[q] = win_hash_slot(v[q]);
+        const uint32_t old = atomicCAS(tab + h[q], kWinHashEmpty, v[q]);
+        left[q] = old != kWinHashEmpty && old != v[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        while (left[q]) {
+            h[q] = (h[q] + 1) & (kWinHashSlots - 1);
+            const uint32_t old = atomicCAS(tab + h[q], kWinHashEmpty, v[q]);
+            left[q] = old != kWinHashEmpty && old != v[q];
+        }
+    }
+}
+
+// Matches among the chunk's elements whose bit is set in `valid` (bit q: g0's
+// component q, bit 4 + q: g1's), as a mask in the same bit order.  No element
+// is kWinHashEmpty.
+__device__ __forceinline__ uint32_t chunk_hash_probe(const uint32_t* tab, const uint4& g0, const uint4& g1,
+                                                     uint32_t valid) {
+    const uint32_t v[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+    uint32_t h[8], hit = 0;
+    bool left[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        h[q] = win_hash_slot(v[q]);
+        const uint32_t t = tab[h[q]];
+        const bool on = (valid >> q) & 1u;
+        hit |= (on && t == v[q] ? 1u : 0u) << q;
+        left[q] = on && t != v[q] && t != kWinHashEmpty;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        while (left[q]) {
+            h[q] = (h[q] + 1) & (kWinHashSlots - 1);
+            const uint32_t t = tab[h[q]];
+            hit |= (t == v[q] ? 1u : 0u) << q;
+            left[q] = t != v[q] && t != kWinHashEmpty;
+        }
+    }
+    return hit;
+}
+
+// Which of the chunk at s.pc this lane probes: stream positions in
+// [v0, s.v1) (the head and tail copies are not elements of their own) whose
+// value is <= hi (the later ones belong to the next window).
+__device__ __forceinline__ uint32_t probe_mask(const SetStream& s, const uint4& g0, const uint4& g1, uint32_t v0,
+                                               uint32_t hi, uint32_t lane) {
+    if ((s.pc != 0 || v0 == 0) && s.pc + kChunk <= s.v1 && s.last <= hi) return 0xffu;
+    uint32_t m = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < 4; ++q) {
+        const uint32_t p0 = s.pc + 4 * lane + q, p1 = p0 + 128;
+        m |= (p0 >= v0 && p0 < s.v1 && comp(g0, q) <= hi ? 1u : 0u) << q;
+        m |= (p1 >= v0 && p1 < s.v1 && comp(g1, q) <= hi ? 1u : 0u) << (4 + q);
+    }
+    return m;
+}
+
+__device__ __forceinline__ bool stream_next(SetStream& s, uint32_t lane) {
+    return s.ph == 0 ? stream_advance<true>(s, lane) : stream_advance<false>(s, lane);
 }
 
 }  // namespace si
