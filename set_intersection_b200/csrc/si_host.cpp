@@ -28,6 +28,7 @@
 #include <cstdint>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -42,7 +43,14 @@ namespace {
 class CopyPool {
 public:
     explicit CopyPool(unsigned threads) {
-        for (unsigned i = 1; i < threads; ++i) workers_.emplace_back([this, i] { loop(i); });
+        workers_.reserve(threads);
+        for (unsigned i = 1; i < threads; ++i) {
+            try {
+                workers_.emplace_back([this, i] { loop(i); });
+            } catch (...) {  // fewer threads than asked for: the caller's share grows
+                break;
+            }
+        }
     }
     ~CopyPool() {
         {
@@ -229,8 +237,8 @@ si_status ensure_staging(si_host_ctx* ctx) {
         SI_CUDA_TRY(cudaEventCreateWithFlags(&ctx->stage_free[k], cudaEventDisableTiming));
     }
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    ctx->pool = new CopyPool(std::min(8u, hw));
-    return SI_OK;
+    ctx->pool = new (std::nothrow) CopyPool(std::min(8u, hw));
+    return ctx->pool ? SI_OK : SI_ERR_UNSUPPORTED;
 }
 
 // bytes from host src to device dst on the context's up stream: directly from
