@@ -779,18 +779,23 @@ si_status batch_tune(const uint32_t* d_elements, const uint64_t* d_offsets, uint
         }
         float ms[kTechCodes] = {};
         for (uint8_t tech = 0; tech < kTechCodes && st == SI_OK; ++tech) {
-            for (int rep = 0; rep < 2 && st == SI_OK; ++rep) {  // the first run warms the caches
+            // three runs: the first warms the caches, the faster of the other two counts
+            ms[tech] = 0.f;
+            for (int rep = 0; rep < 3 && st == SI_OK; ++rep) {
                 cudaEventRecord(e0, stream);
                 st = batch_launch(d_elements, d_offsets, k, d_pairs, npairs, T, tech, d_subset, m.size(), d_counts,
                                   ws, ws_bytes, stream);
                 cudaEventRecord(e1, stream);
+                if (st != SI_OK || rep == 0) continue;
+                if (cudaEventSynchronize(e1) != cudaSuccess) {
+                    st = cuda_fail(cudaGetLastError(), "batch_tune");
+                    break;
+                }
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                ms[tech] = rep == 1 ? t : std::min(ms[tech], t);
             }
             if (st != SI_OK) break;
-            if (cudaEventSynchronize(e1) != cudaSuccess) {
-                st = cuda_fail(cudaGetLastError(), "batch_tune");
-                break;
-            }
-            cudaEventElapsedTime(&ms[tech], e0, e1);
         }
         if (st != SI_OK) break;
         // another technique replaces the default only when it is 3 % faster
