@@ -157,40 +157,46 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 }
 
 // ------------------------------------------------------ incidence build --
-// One CTA per (row, 32 KiB column chunk): the chunk is assembled in shared
-// memory (zeros, then a `one` byte at every element of the set inside the
-// chunk) and written out with 16-byte stores; rows >= k are all zero.
+// One CTA per row of M: the row is assembled in shared memory 32 KiB of
+// columns at a time (zeros, then a `one` byte at every element of the set
+// inside the chunk) and written out with 16-byte stores; rows >= k are all
+// zero.  The set is read once, in order: each chunk's loop stops at the first
+// element past the chunk, which is where the next chunk starts.
 constexpr uint32_t kChunk = 32768;
 __global__ void __launch_bounds__(256) build_incidence_kernel(const uint32_t* __restrict__ elements,
                                                               const uint64_t* __restrict__ offsets, uint32_t k,
                                                               uint8_t* __restrict__ M, uint64_t row_bytes,
                                                               uint32_t universe, uint8_t one, uint32_t* err) {
     __shared__ __align__(16) uint8_t chunk[kChunk];
+    __shared__ unsigned long long s_next;
     const uint32_t row = blockIdx.x;
-    const uint64_t c0 = static_cast<uint64_t>(blockIdx.y) * kChunk;
     uint4* c4 = reinterpret_cast<uint4*>(chunk);
-    for (uint32_t x = threadIdx.x; x < kChunk / 16; x += blockDim.x) c4[x] = make_uint4(0, 0, 0, 0);
-    __syncthreads();
+    uint64_t lo = 0, e = 0;
     if (row < k) {
-        const uint64_t s = offsets[row], e = offsets[row + 1];
-        // first element >= c0 (binary search, the set is ascending)
-        uint64_t lo = s, hi = e;
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (__ldg(elements + mid) < c0) lo = mid + 1; else hi = mid;
-        }
+        lo = offsets[row];
+        e = offsets[row + 1];
+    }
+    for (uint64_t c0 = 0; c0 < row_bytes; c0 += kChunk) {
+        const uint64_t rem = row_bytes - c0;
+        const uint32_t n16 = static_cast<uint32_t>((rem < kChunk ? rem : kChunk) / 16);
+        for (uint32_t x = threadIdx.x; x < n16; x += blockDim.x) c4[x] = make_uint4(0, 0, 0, 0);
+        if (threadIdx.x == 0) s_next = e;
+        __syncthreads();
         for (uint64_t x = lo + threadIdx.x; x < e; x += blockDim.x) {
             const uint64_t v = __ldg(elements + x);
-            if (v >= c0 + kChunk) break;
+            if (v >= c0 + kChunk) {  // this thread's first element past the chunk
+                atomicMin(&s_next, static_cast<unsigned long long>(x));
+                break;
+            }
             if (v < c0 || v > universe) { record_error(err, SI_ERR_INVALID_INPUT, 20, row); continue; }
             chunk[v - c0] = one;
         }
+        __syncthreads();
+        uint4* dst = reinterpret_cast<uint4*>(M + static_cast<uint64_t>(row) * row_bytes + c0);
+        for (uint32_t x = threadIdx.x; x < n16; x += blockDim.x) dst[x] = c4[x];
+        lo = s_next;
+        __syncthreads();  // the chunk and s_next are rewritten for the next columns
     }
-    __syncthreads();
-    uint4* dst = reinterpret_cast<uint4*>(M + static_cast<uint64_t>(row) * row_bytes + c0);
-    const uint64_t rem = row_bytes - c0;
-    const uint32_t n16 = static_cast<uint32_t>((rem < kChunk ? rem : kChunk) / 16);
-    for (uint32_t x = threadIdx.x; x < n16; x += blockDim.x) dst[x] = c4[x];
 }
 
 // ----------------------------------------------------- tensor-core GEMM --
@@ -460,8 +466,7 @@ si_status misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, uint
     uint8_t* M = reinterpret_cast<uint8_t*>(w + L.off_matrix);
     {
         PhaseTimer timer("mm_incidence", stream);
-        dim3 grid(L.k_pad, static_cast<unsigned>((L.row_bytes + kChunk - 1) / kChunk));
-        build_incidence_kernel<<<grid, 256, 0, stream>>>(d_elements, d_offsets, k, M, L.row_bytes, universe,
+        build_incidence_kernel<<<L.k_pad, 256, 0, stream>>>(d_elements, d_offsets, k, M, L.row_bytes, universe,
                                                          fp8 ? uint8_t(0x38) : uint8_t(1), err);  // 1.0 in e4m3 = 0x38
     }
     SI_LAUNCH_CHECK("build_incidence_kernel");
