@@ -24,14 +24,20 @@ Metric: Gelem/s = (|A| + |B|) / step time.
           (via api.intersect_host): pinned host sets -> H2D -> kernels ->
           count + elements D2H, per step, pipelined over 8 value ranges.
   roofline  live per-launch time of the dominant kernel (the tile kernel) from the
-          library's phase timer over the timed region, against measured HBM;
-          phase_avg_ms lists every phase of the step (set-up, stream/tiles, copy).
+          library's phase timer, against measured HBM; phase_avg_ms lists every
+          phase of the step (set-up, stream/tiles, copy).  The phase events are
+          recorded in a second pass of the same steps (phase_pass): between the
+          launches they hold back the programmatic dependent launches, so the
+          value pass runs without them.
   cpu_baseline  the reference's own CPU executable (oracle/_ref/stdintersection,
           built from the reference sources) on value-range slices of the same
           pair, timed by the reference's HostTimer.
   --impl reference  the same executable on slices of the same pair, built
           in that process by the oracle's restatement of the engine's seeded
           generator (the engine's library is never loaded there).
+  techniques  (SISI, one GPU) every technique on the same pair after the timed
+          region, 20 steps each, with whether its count and elements equal the
+          benchmarked call's.
 
 Multi-GPU: the single-pair path is replicas only -- each rank runs its own
 independent pair (no data-path collective); value is the whole-job aggregate.
@@ -351,8 +357,6 @@ def run_ours(args, rank: int, world: int):
     rep.barrier()
     torch.cuda.synchronize()
 
-    lib.si_timer_reset()
-    lib.si_timer_enable(1)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev.index) as clocks:
         start.record(stream)
@@ -360,13 +364,28 @@ def run_ours(args, rank: int, world: int):
             step()
         stop.record(stream)
         stop.synchronize()
-    lib.si_timer_enable(0)
     ms_total = start.elapsed_time(stop)
+    # per-kernel times: a second pass of the same steps with the library's
+    # phase events recorded around every launch.  Those records sit between
+    # the launches (a kernel launched as a programmatic dependent then waits
+    # for the one before it to finish), so value comes from the pass without
+    # them.
+    phase_steps = max(1, min(args.steps, 50))
+    lib.si_timer_reset()
+    lib.si_timer_enable(1)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(phase_steps):
+        step()
+    p1.record(stream)
+    p1.synchronize()
+    lib.si_timer_enable(0)
+    phase_pass_ms = p0.elapsed_time(p1) / phase_steps
     tile_ms, tile_n = ctypes.c_double(0), ctypes.c_uint64(0)
     lib.si_timer_read(b"sisi_tile", ctypes.byref(tile_ms), ctypes.byref(tile_n))
     phases = {}
     for ph in ("sisi_split", "sisi_tile", "sisi_scan", "sisi_copy", "obs_sample", "obs_search",
-               "obs_scan", "obs_compact"):
+               "obs_compact"):
         p_ms, p_n = ctypes.c_double(0), ctypes.c_uint64(0)
         lib.si_timer_read(ph.encode(), ctypes.byref(p_ms), ctypes.byref(p_n))
         if p_n.value:
@@ -426,6 +445,30 @@ def run_ours(args, rank: int, world: int):
                            "steps": p_steps}
         assert cp == c
 
+    # ---- every technique on the same pair (outside the timed region) ----
+    techniques = None
+    if world == 1 and not args.no_techniques:
+        techniques = {}
+        t_steps = max(1, min(args.steps, 20))
+        want_out = out[:c].clone() if out is not None else None
+        tcount = torch.zeros(1, dtype=torch.int64, device=dev)
+        for tech in ("auto", "ip", "obs", "hi", "bitmap"):
+            for _ in range(3):
+                api.sisi_into(da, db, tcount, out, ws, tech, stream)
+            ws.check(stream)
+            same = int(tcount.item()) == c and (out is None or bool(torch.equal(out[:c], want_out)))
+            t0e, t1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0e.record(stream)
+            for _ in range(t_steps):
+                api.sisi_into(da, db, tcount, out, ws, tech, stream)
+            t1e.record(stream)
+            t1e.synchronize()
+            t_ms = t0e.elapsed_time(t1e) / t_steps
+            techniques[tech] = {"ms_per_step": t_ms, "value": (n_a + n_b) / (t_ms * 1e6), "unit": "Gelem/s",
+                                "steps": t_steps, "same_result": same}
+            log(f"technique {tech}: {t_ms:.4f} ms per step, same result: {same}")
+        del want_out
+
     if rank != 0:
         rep.close()
         return
@@ -444,7 +487,7 @@ def run_ours(args, rank: int, world: int):
         "ip": ("ip_tile_kernel<merge path>", 3),
         "hi": ("bh_stream_kernel", 2 if args.materialize else 1),
         "bitmap": ("bp_stream_kernel", 2 if args.materialize else 1),
-        "obs": ("obs_search_kernel", 4 if args.materialize else 2),
+        "obs": ("obs_search_kernel", 3 if args.materialize else 2),
     }[engine]
     if engine == "obs":
         tile_avg_ms = phases.get("obs_search")
@@ -469,12 +512,17 @@ def run_ours(args, rank: int, world: int):
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": kernel, "engine": engine, "alg_bytes_per_launch": alg_bytes,
                      "avg_launch_ms": tile_avg_ms, "launches": int(tile_n.value), "peak_source": peak_src,
-                     "phase_avg_ms": phases},
+                     "phase_avg_ms": phases,
+                     "phase_pass": {"steps": phase_steps, "ms_per_step": phase_pass_ms,
+                                    "note": "launch and phase times from a second pass with the phase events "
+                                            "recorded around every launch"}},
         "e2e": e2e,
         "gpu_launches": launches * args.steps,
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
     }
+    if techniques is not None:
+        line["techniques"] = techniques
     if world == 1 and not args.no_extras:
         line["other_workloads"] = other_workloads(args)
     print(json.dumps(line), flush=True)
@@ -1058,7 +1106,7 @@ def other_workloads(args) -> list:
         cfg = d.get("config") or {}
         keep = {k: cfg[k] for k in ("technique", "operand", "parity_vs_oracle", "speedup_vs_plain",
                                      "plain_popcount_ms_per_step", "plain_per_pair") if k in cfg}
-        keep.update({k: d[k] for k in ("technique", "parity_vs_oracle") if k in d})
+        keep.update({k: d[k] for k in ("technique", "parity_vs_oracle", "techniques") if k in d})
         out.append({"workload": wl, "metric": d["metric"], "value": d["value"], "unit": d["unit"],
                     "ms_per_step": d["ms_per_step"], "steps": d["steps"],
                     "roofline": {k: roof.get(k) for k in ("bound", "achieved", "peak", "unit", "frac", "kernel",
@@ -1087,6 +1135,8 @@ def main():
     p.add_argument("--no-plain", action="store_true",
                    help="dense / batch: skip timing the plain kernel (popcount / one call per pair)")
     p.add_argument("--dtype", choices=["int8", "fp8"], default="int8", help="dense: tensor-core operand type")
+    p.add_argument("--no-techniques", action="store_true",
+                   help="SISI: skip timing every technique on the workload's pair (outside the timed region)")
     p.add_argument("--no-extras", action="store_true",
                    help="SISI at N=1: skip the short runs of the other workloads added to the line")
     args = p.parse_args()

@@ -316,10 +316,12 @@ si_status si_misi_dense(const uint32_t* d_elements, const uint64_t* d_offsets, u
  * "sisi_split", "sisi_tile", and for BITMAP with elements "sisi_scan",
  * "sisi_copy"; dense all pairs "mm_incidence", "mm_gemm",
  * "naive_bitmaps", "naive_popcount"; all pairs of a tile "misi_plan",
- * "misi_probe"; single pair by search "obs_sample", "obs_search", "obs_scan",
- * "obs_compact"; batched pairs "batch_plan", "batch_count".  si_timer_read synchronises on
- * the recorded events and returns the summed milliseconds and the number of
- * launches of one phase.
+ * "misi_probe"; single pair by search "obs_sample", "obs_search" (with the
+ * offsets scan when elements are written), "obs_compact"; batched pairs
+ * "batch_plan", "batch_count".  The events come from a pool that
+ * si_timer_reset refills, so a timed launch costs two event records.
+ * si_timer_read synchronises on the recorded events and returns the summed
+ * milliseconds and the number of launches of one phase.
  */
 void si_timer_enable(int on);
 void si_timer_reset(void);

@@ -37,12 +37,28 @@ int sm_count() {
 namespace {
 
 struct TimerRecord {
-    std::string name;
+    const char* name = nullptr;  // the launcher's string literal
     cudaEvent_t start = nullptr, stop = nullptr;
+    int device = 0;
 };
 std::mutex g_timer_mu;
 bool g_timer_on = false;
 std::vector<TimerRecord> g_timer;
+// Idle events with their device: si_timer_reset returns the records' events
+// here, so a timed launch records two events instead of creating them.
+std::vector<std::pair<int, cudaEvent_t>> g_event_pool;
+
+cudaEvent_t pool_take_locked(int dev) {
+    for (size_t i = g_event_pool.size(); i-- > 0;) {
+        if (g_event_pool[i].first != dev) continue;
+        const cudaEvent_t e = g_event_pool[i].second;
+        g_event_pool[i] = g_event_pool.back();
+        g_event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    return cudaEventCreate(&e) == cudaSuccess ? e : nullptr;
+}
 
 }  // namespace
 
@@ -51,9 +67,12 @@ PhaseTimer::PhaseTimer(const char* name, cudaStream_t stream) : slot_(-1), strea
     if (!g_timer_on) return;
     TimerRecord r;
     r.name = name;
-    if (cudaEventCreate(&r.start) != cudaSuccess) return;
-    if (cudaEventCreate(&r.stop) != cudaSuccess) {
-        cudaEventDestroy(r.start);
+    if (cudaGetDevice(&r.device) != cudaSuccess) return;
+    r.start = pool_take_locked(r.device);
+    if (!r.start) return;
+    r.stop = pool_take_locked(r.device);
+    if (!r.stop) {
+        g_event_pool.emplace_back(r.device, r.start);
         return;
     }
     cudaEventRecord(r.start, stream);
@@ -71,8 +90,8 @@ namespace {
 
 void timer_clear_locked() {
     for (auto& r : g_timer) {
-        cudaEventDestroy(r.start);
-        cudaEventDestroy(r.stop);
+        g_event_pool.emplace_back(r.device, r.start);
+        g_event_pool.emplace_back(r.device, r.stop);
     }
     g_timer.clear();
 }
@@ -355,7 +374,7 @@ si_status si_timer_read(const char* phase, double* total_ms, uint64_t* launches)
     double sum = 0.0;
     uint64_t n = 0;
     for (auto& r : si::g_timer) {
-        if (r.name != phase) continue;
+        if (std::strcmp(r.name, phase) != 0) continue;
         SI_CUDA_TRY(cudaEventSynchronize(r.stop));
         float ms = 0.f;
         SI_CUDA_TRY(cudaEventElapsedTime(&ms, r.start, r.stop));

@@ -30,6 +30,26 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Launches `kernel` with programmatic stream serialization: it may start while
+// the previous kernel on the stream finishes, and must execute
+// griddepcontrol.wait before it reads that kernel's results (or writes what
+// that kernel still reads).
+template <class Kernel, class... Args>
+si_status launch_dependent(Kernel kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SI_CUDA_TRY(cudaLaunchKernelEx(&cfg, kernel, args...));
+    return SI_OK;
+}
+
 // Named phase timing on the launching stream (the engine's counterpart of the
 // reference's DeviceTimer, include/device_timer.cuh:20-78).  When enabled via
 // si_timer_enable, PhaseTimer records a cudaEvent pair around a launch.

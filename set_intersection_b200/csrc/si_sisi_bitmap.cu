@@ -490,25 +490,6 @@ BpLayout make_bp_layout(uint64_t nA, uint64_t nB) {
     return L;
 }
 
-// Launches `kernel` with programmatic stream serialization: it may start while
-// the previous kernel on the stream finishes, and waits for it (griddepcontrol.wait)
-// before reading that kernel's results.
-template <class Kernel, class... Args>
-si_status launch_dependent(Kernel kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    SI_CUDA_TRY(cudaLaunchKernelEx(&cfg, kernel, args...));
-    return SI_OK;
-}
-
 }  // namespace
 
 si_status pivot_split(const uint32_t* dA, uint64_t nA, const uint32_t* dB, uint64_t nB, uint64_t S,

@@ -266,3 +266,27 @@ def test_intersect_host_pipeline(cuda, tech, chunks):
         c, got = api.intersect_host(ha, hb, tech, ctx=ctx, chunks=chunks)
         assert c == want.size
         assert np.array_equal(got.numpy().view(np.uint32), want)
+
+
+@pytest.mark.parametrize("n_small", [1, 7, 100, 18944, 18945, 37888, 37889, 75776, 75777, 400000, 700000,
+                                     3000000])
+def test_obs_lane_groups_and_chunking(cuda, n_small):
+    """obs at sizes either side of each change of lanes per element (8, 4, 2,
+    1 on 148 SMs) and of mask words per warp, with planted hits, the values 0
+    and 2^32 - 1, and larger sets whose sample stride T is 1, a few and large."""
+    rng = np.random.default_rng(n_small)
+    for n_large in (5000, 8192 * 3 + 5, 1 << 22):
+        n_large = max(n_large, n_small)
+        big = _u(rng, n_large, 1 << 31)
+        big[0], big[-1] = 0, 0xFFFFFFFF
+        big = np.unique(big)
+        pool = np.unique(np.concatenate([
+            rng.choice(big, size=n_small // 3 + 1, replace=False),
+            rng.integers(0, 1 << 32, size=n_small + 16, dtype=np.uint64).astype(np.uint32)]))
+        pool = pool[(pool != 0) & (pool != 0xFFFFFFFF)]
+        # exactly n_small elements: 0, 2^32 - 1 and n_small - 2 of the pool
+        small = np.sort(np.concatenate([np.array([0, 0xFFFFFFFF], dtype=np.uint32)[: min(2, n_small)],
+                                        rng.choice(pool, size=max(0, n_small - 2), replace=False)]))
+        assert small.size == n_small
+        check(small, big, "obs")
+        check(big, small, "obs")
