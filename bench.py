@@ -1081,19 +1081,19 @@ def run_ours_batch(args, rank: int, world: int):
 
 
 # Short runs of the other configurations, for the record of a default run.
-EXTRAS = [
-    ("misi_dense", ["--technique", "mm", "--dtype", "int8"]),
-    ("misi_dense", ["--technique", "mm", "--dtype", "fp8", "--no-plain"]),
-    ("misi_powerlaw", ["--technique", "bitmap"]),
-    ("batch_pairs", ["--technique", "auto"]),
-    ("sisi_skewed", ["--technique", "auto"]),
+EXTRAS = [  # workload, arguments, timed steps
+    ("misi_dense", ["--technique", "mm", "--dtype", "int8"], 5),
+    ("misi_dense", ["--technique", "mm", "--dtype", "fp8", "--no-plain"], 5),
+    ("misi_powerlaw", ["--technique", "bitmap"], 5),
+    ("batch_pairs", ["--technique", "auto"], 5),
+    ("sisi_skewed", ["--technique", "auto"], 200),  # 0.03 ms steps
 ]
 
 
 def other_workloads(args) -> list:
     out = []
-    for wl, extra in EXTRAS:
-        cmd = [sys.executable, os.path.abspath(__file__), "--workload", wl, "--steps", "5", "--warmup", "3",
+    for wl, extra, steps in EXTRAS:
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", wl, "--steps", str(steps), "--warmup", "3",
                "--no-e2e", "--no-cpu-baseline", "--no-extras", *extra]
         t0 = time.time()
         try:
