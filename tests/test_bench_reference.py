@@ -48,3 +48,19 @@ def test_reference_pair_equals_engine_pair(tmp_path, monkeypatch):
     monkeypatch.setattr(bench, "CACHE_DIR", str(tmp_path / "eng"))
     a2, b2 = bench.make_pair("sisi_plain")
     assert (a == a2).all() and (b == b2).all()
+
+
+def test_extras_and_flags_are_well_formed():
+    """Every short run a default bench adds names a known workload with a
+    positive step count, and the SISI flags parse."""
+    sys.path.insert(0, ROOT)
+    import bench
+    for wl, extra, steps in bench.EXTRAS:
+        assert wl in bench.WORKLOADS
+        assert isinstance(steps, int) and steps >= 1
+        assert "--technique" in extra
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"], capture_output=True, text=True,
+                       timeout=120, cwd=ROOT)
+    assert r.returncode == 0
+    for flag in ("--no-techniques", "--no-extras", "--bucket-times", "--count-only"):
+        assert flag in r.stdout
